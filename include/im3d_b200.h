@@ -1,0 +1,178 @@
+/*
+ * im3d_b200.h -- C ABI of the B200 (sm_100a) backend for 3dimagetoolkit's
+ * RSFE Split-Bregman level-set segmentation path.
+ *
+ * Every entry point returns an int status (IM3D_OK = 0). No C++ types, no torch
+ * types cross this boundary: plain pointers, sizes and POD structs only.
+ *
+ * Volumes follow the reference's image3d layout (header/image3d_imp.hxx:142-153):
+ * element (i, j, k) of an nx x ny x nz volume sits at index (i*ny + j)*nz + k, so k
+ * is the contiguous axis. Spacings are hx, hy, hz.
+ *
+ * Pointer arguments may be host memory (pageable or pinned) or device memory of
+ * the context's device; the library asks the CUDA runtime which one each pointer
+ * is and stages host buffers through device buffers that the context owns. All
+ * calls on one context are serialised on the context's stream and return after
+ * the results are in the caller's buffers.
+ *
+ * Status codes map to the reference's WARNING behaviour: the reference prints a
+ * WARNING and returns (e.g. image3d_imp.hxx:221-225, rsfe_splitbregman_imp.hxx:957-960);
+ * here the call returns a non-zero status and im3d_ctx_last_error() holds the text.
+ */
+#ifndef IM3D_B200_H
+#define IM3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IM3D_OK 0
+#define IM3D_ERR_INVALID_ARG 1   /* bad size, spacing or parameter */
+#define IM3D_ERR_UNSUPPORTED 2   /* 2-D volumes (nz == 1) and dims < 3: not on this backend */
+#define IM3D_ERR_NOT_CONVERGED 3 /* a sweep cap was hit before the requested tolerance */
+#define IM3D_ERR_CUDA 4          /* a CUDA runtime call failed (text in last_error) */
+#define IM3D_ERR_OOM 5           /* device allocation failed */
+#define IM3D_ERR_NO_DEVICE 6     /* no usable sm_100 device */
+
+/* Boundary condition selector. The reference keeps bc_type private
+ * (rsfe_splitbregman.hxx:108); its constructor sets bc = NEU but installs
+ * DirGaussSeidel (rsfe_splitbregman_imp.hxx:33-35), so an untouched instance solves
+ * with Dirichlet value 0. IM3D_BC_DEFAULT reproduces that; NEU and DIR reproduce
+ * set_bc(NEU) / set_bc(DIR) (rsfe_splitbregman_imp.hxx:1294-1322). */
+#define IM3D_BC_DEFAULT 0
+#define IM3D_BC_NEU 1
+#define IM3D_BC_DIR 2
+
+/* Order of the Gauss-Seidel point updates inside one sweep.
+ * LEXICOGRAPHIC reproduces lapl::DirGaussSeidel / lapl::NeuGaussSeidel exactly
+ * (poisson_imp.hxx:340-429 / 23-336): every point sees new values at its minus
+ * neighbours and old values at its plus neighbours. REDBLACK updates the points
+ * with even (i+j+k) first, then the odd ones, with the same per-point formula. */
+#define IM3D_SWEEP_LEXICOGRAPHIC 0
+#define IM3D_SWEEP_REDBLACK 1
+
+/* Parameters of segm::rsfe_splitbregman<T> (rsfe_splitbregman.hxx:99-894).
+ * im3d_rsfe_params_default() fills the reference constructor's values
+ * (rsfe_splitbregman_imp.hxx:25-41). Field names are the reference's. */
+typedef struct im3d_rsfe_params {
+    double tol;                 /* outer stop: ||phi-phiold||_L2/||phiold||_L2 <= tol (1e-5) */
+    double sigma;               /* Gaussian std-dev of the fitting kernel (3) */
+    double lamda;               /* Bregman weight (5e-2) */
+    double lamda1;              /* inside fitting weight (1e-5) */
+    double lamda2;              /* outside fitting weight (1e-5) */
+    double beta;                /* edge detector g = 1/(1+beta|grad u0|^2) (100) */
+    double nu;                  /* TV weight (1) */
+    double dt;                  /* pseudo time step of the unsteady Poisson step (1) */
+    double epsilon;             /* Heaviside width (1e-3) */
+    double a0;                  /* lower level-set value (0) */
+    double b0;                  /* upper level-set value (1) */
+    double ls_tol;              /* relative-change stop of the sweep loop, 0 = off (0) */
+    double edge_detector_sigma; /* pre-blur of u0 for the edge detector, 0 = none (0) */
+    /* extensions with no reference counterpart */
+    double gs_rel_res_tol;      /* >0: each outer iteration solves (1/dt - Lap) u = u_old/dt + rhs
+                                   to this relative residual instead of running ls_steps sweeps */
+    double omega;               /* over-relaxation factor of the residual solve (1 = Gauss-Seidel) */
+    int32_t maxiter;            /* outer iteration cap (100) */
+    int32_t ls_steps;           /* sweeps per outer iteration (5) */
+    int32_t bc;                 /* IM3D_BC_* (IM3D_BC_DEFAULT) */
+    int32_t gaussian_pixel_approach; /* build the Gaussian with unit spacing (0) */
+    int32_t init_variables;     /* reset b and div(d-b) after the first iteration (0) */
+    int32_t sweep;              /* IM3D_SWEEP_* used by the ls_steps sweeps (LEXICOGRAPHIC) */
+    int32_t gs_max_sweeps;      /* sweep cap of the residual solve (1000) */
+    int32_t gs_check_every;     /* residual evaluated every this many sweeps (2) */
+} im3d_rsfe_params;
+
+typedef struct im3d_rsfe_stats {
+    double last_tol;      /* ||phi-phiold||_L2/||phiold||_L2 of the last outer iteration */
+    double last_rel_res;  /* relative residual at the end of the last solve (residual mode) */
+    double last_ls_err;   /* relative change of the last sweep (ls_tol mode) */
+    double setup_ms;      /* device time of the set-up (filters, k*1, k*u0, edge detector) */
+    double loop_ms;       /* device time of the outer loop */
+    int64_t total_sweeps; /* sweeps over all outer iterations */
+    int32_t iterations;   /* outer iterations run */
+    int32_t last_sweeps;  /* sweeps of the last outer iteration */
+    int32_t not_converged;/* outer iterations whose solve hit gs_max_sweeps */
+    int32_t reserved;
+} im3d_rsfe_stats;
+
+typedef struct im3d_ctx im3d_ctx;
+
+/* Context: one per host thread; owns a stream, device buffers and cached plans. */
+int im3d_ctx_create(int device, im3d_ctx** out);
+int im3d_ctx_destroy(im3d_ctx* ctx);
+const char* im3d_ctx_last_error(const im3d_ctx* ctx);
+/* Run subsequent calls on an external cudaStream_t (NULL = the context's own). */
+int im3d_ctx_set_stream(im3d_ctx* ctx, void* cuda_stream);
+/* Count of kernel launches the context issued since creation (instrumentation). */
+int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
+
+/* Reference constructor defaults (rsfe_splitbregman_imp.hxx:25-41) plus the
+ * extension defaults documented in im3d_rsfe_params. */
+void im3d_rsfe_params_default(im3d_rsfe_params* p);
+
+/* Gaussian filtering with zero boundary:
+ * conv::filtering<T>::build_gaussian_filter(f, sigma, radius, pixel_approach)
+ * (convolution_imp.hxx:22-91) followed by conv::acyclic_fftw_convolution(out, in)
+ * (convolution_imp.hxx:535-653). The result is the linear convolution with the
+ * normalised kernel, cropped to the input size; computed here as three 1-D passes. */
+int im3d_gauss_filter_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
+                          double hx, double hy, double hz, double sigma, double radius,
+                          int pixel_approach);
+int im3d_gauss_filter_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
+                          double hx, double hy, double hz, double sigma, double radius,
+                          int pixel_approach);
+
+/* `sweeps` calls of lapl::DirGaussSeidel (bc_type DIR or DEFAULT) or
+ * lapl::NeuGaussSeidel (NEU), in place on res (poisson_imp.hxx:340-429, 23-336):
+ * res <- (sum of neighbour terms + b + res/dt) * htilde, boundary per bc_type. */
+int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,
+                            double hx, double hy, double hz, double dt, double bc, int bc_type,
+                            int sweep_order, int sweeps);
+int im3d_poisson_sweeps_f64(im3d_ctx* ctx, double* res, const double* b, int nx, int ny, int nz,
+                            double hx, double hy, double hz, double dt, double bc, int bc_type,
+                            int sweep_order, int sweeps);
+
+/* Red-black solve of (1/dt - Lap_h) u = u_in/dt + b (u_in = u on entry, held fixed),
+ * boundary per bc_type, until ||residual||_2/||b + u_in/dt||_2 <= rel_res_tol (checked
+ * every check_every sweeps) or max_sweeps; returns IM3D_ERR_NOT_CONVERGED at the cap. */
+int im3d_poisson_solve_f32(im3d_ctx* ctx, float* u, const float* b, int nx, int ny, int nz,
+                           double hx, double hy, double hz, double dt, double bc, int bc_type,
+                           double rel_res_tol, int max_sweeps, int check_every, double omega,
+                           int* sweeps_done, double* rel_res);
+int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, int ny, int nz,
+                           double hx, double hy, double hz, double dt, double bc, int bc_type,
+                           double rel_res_tol, int max_sweeps, int check_every, double omega,
+                           int* sweeps_done, double* rel_res);
+
+/* image3d<T>::grad (image3d_imp.hxx:744-889): out holds 3 volumes, component-major. */
+int im3d_grad_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
+                  double hx, double hy, double hz);
+int im3d_grad_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
+                  double hx, double hy, double hz);
+/* im3d::div (image3d_imp.hxx:948-1384): in holds 3 volumes, component-major. */
+int im3d_div_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
+                 double hx, double hy, double hz);
+int im3d_div_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
+                 double hx, double hy, double hz);
+
+/* segm::rsfe_splitbregman<T>::apply(myim, init) (rsfe_splitbregman_imp.hxx:1547-1995);
+ * init == NULL is apply(myim) with the default cube (:1531-1543, :48-95).
+ * phi_out receives getoutput() (segmentation.hxx:108-111). u_out (phi after the last
+ * solve, before the clamp), f1_out and f2_out (the last iteration's fitting means,
+ * :1709-1717) are optional (NULL = not copied). */
+int im3d_rsfe_apply_f32(im3d_ctx* ctx, const float* myim, const float* init, int nx, int ny,
+                        int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
+                        float* phi_out, float* u_out, float* f1_out, float* f2_out,
+                        im3d_rsfe_stats* stats);
+int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, int nx, int ny,
+                        int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
+                        double* phi_out, double* u_out, double* f1_out, double* f2_out,
+                        im3d_rsfe_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IM3D_B200_H */
