@@ -1,0 +1,259 @@
+"""ctypes binding of the C ABI in include/im3d_b200.h (libim3d_b200.so).
+
+The shared library is built in-tree by ``__graft_entry__.build()`` (nvcc, sm_100a).
+There is no CPU fallback: if the library or a CUDA device is missing, every entry
+point raises.
+
+Arrays may be numpy arrays (host memory; the library stages them through its own
+device buffers) or CUDA torch tensors (device memory, used in place). float32 calls
+the ``_f32`` entry points, float64 the ``_f64`` ones.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libim3d_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "im3d_b200.h")
+
+OK = 0
+ERR_INVALID_ARG = 1
+ERR_UNSUPPORTED = 2
+ERR_NOT_CONVERGED = 3
+ERR_CUDA = 4
+ERR_OOM = 5
+ERR_NO_DEVICE = 6
+
+BC_DEFAULT, BC_NEU, BC_DIR = 0, 1, 2
+SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK = 0, 1
+
+_STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "NOT_CONVERGED", 4: "CUDA",
+                 5: "OOM", 6: "NO_DEVICE"}
+
+
+class Im3dError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class RsfeParams(C.Structure):
+    """``im3d_rsfe_params``: the parameters of segm::rsfe_splitbregman<T>."""
+
+    _fields_ = [
+        ("tol", C.c_double), ("sigma", C.c_double), ("lamda", C.c_double),
+        ("lamda1", C.c_double), ("lamda2", C.c_double), ("beta", C.c_double),
+        ("nu", C.c_double), ("dt", C.c_double), ("epsilon", C.c_double),
+        ("a0", C.c_double), ("b0", C.c_double), ("ls_tol", C.c_double),
+        ("edge_detector_sigma", C.c_double), ("gs_rel_res_tol", C.c_double),
+        ("omega", C.c_double),
+        ("maxiter", C.c_int32), ("ls_steps", C.c_int32), ("bc", C.c_int32),
+        ("gaussian_pixel_approach", C.c_int32), ("init_variables", C.c_int32),
+        ("sweep", C.c_int32), ("gs_max_sweeps", C.c_int32), ("gs_check_every", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class RsfeStats(C.Structure):
+    _fields_ = [
+        ("last_tol", C.c_double), ("last_rel_res", C.c_double), ("last_ls_err", C.c_double),
+        ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_sweeps", C.c_int64),
+        ("iterations", C.c_int32), ("last_sweeps", C.c_int32), ("not_converged", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded libim3d_b200.so; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        L.im3d_ctx_last_error.restype = C.c_char_p
+        L.im3d_ctx_launch_count.restype = C.c_int64
+        L.im3d_rsfe_params_default.restype = None
+        _lib = L
+    return _lib
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Names of the functions declared in include/im3d_b200.h."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(im3d_[a-z0-9_]+)\s*\(", text)))
+
+
+def default_params(**overrides) -> RsfeParams:
+    """Reference constructor defaults (rsfe_splitbregman_imp.hxx:25-41), then overrides."""
+    p = RsfeParams()
+    lib().im3d_rsfe_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a):
+    """(void*, dtype) of a numpy array or a CUDA torch tensor; None passes NULL."""
+    if a is None:
+        return None, None
+    if _is_torch(a):
+        import torch
+
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        dt = {torch.float32: np.float32, torch.float64: np.float64}[a.dtype]
+        return C.c_void_p(a.data_ptr()), dt
+    if not isinstance(a, np.ndarray) or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous numpy array or a CUDA tensor")
+    return C.c_void_p(a.ctypes.data), a.dtype.type
+
+
+def _suffix(dt) -> str:
+    if dt == np.float32:
+        return "f32"
+    if dt == np.float64:
+        return "f64"
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _empty_like(a, shape=None):
+    shape = tuple(a.shape) if shape is None else tuple(shape)
+    if _is_torch(a):
+        import torch
+
+        return torch.empty(shape, dtype=a.dtype, device=a.device)
+    return np.empty(shape, dtype=a.dtype)
+
+
+class Context:
+    """One im3d_ctx: a CUDA stream, device buffers reused across calls."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        st = lib().im3d_ctx_create(C.c_int(device), C.byref(self._h))
+        if st != OK:
+            raise Im3dError(st, f"im3d_ctx_create(device={device}) failed")
+        self.device = device
+
+    def close(self):
+        if self._h:
+            lib().im3d_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def launches(self) -> int:
+        return int(lib().im3d_ctx_launch_count(self._h))
+
+    def last_error(self) -> str:
+        return lib().im3d_ctx_last_error(self._h).decode()
+
+    def _check(self, st: int, allow=()):
+        if st != OK and st not in allow:
+            raise Im3dError(st, self.last_error())
+        return st
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(lib().im3d_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    # -- operators -----------------------------------------------------------
+    def gauss_filter(self, x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, out=None):
+        px, dt = _ptr(x)
+        out = _empty_like(x) if out is None else out
+        po, _ = _ptr(out)
+        fn = getattr(lib(), "im3d_gauss_filter_" + _suffix(dt))
+        self._check(fn(self._h, px, po, *map(C.c_int, x.shape), *map(C.c_double, h),
+                       C.c_double(sigma), C.c_double(radius), C.c_int(int(pixel_approach))))
+        return out
+
+    def grad(self, x, h=(1.0, 1.0, 1.0)):
+        px, dt = _ptr(x)
+        out = _empty_like(x, (3,) + tuple(x.shape))
+        po, _ = _ptr(out)
+        fn = getattr(lib(), "im3d_grad_" + _suffix(dt))
+        self._check(fn(self._h, px, po, *map(C.c_int, x.shape), *map(C.c_double, h)))
+        return out
+
+    def div(self, v, h=(1.0, 1.0, 1.0)):
+        pv, dt = _ptr(v)
+        out = _empty_like(v, tuple(v.shape[1:]))
+        po, _ = _ptr(out)
+        fn = getattr(lib(), "im3d_div_" + _suffix(dt))
+        self._check(fn(self._h, pv, po, *map(C.c_int, out.shape), *map(C.c_double, h)))
+        return out
+
+    def poisson_sweeps(self, res, b, dt=1.0, bc=0.0, bc_type=BC_DIR, order=SWEEP_LEXICOGRAPHIC,
+                       sweeps=1, h=(1.0, 1.0, 1.0)):
+        """In place on ``res``: DirGaussSeidel / NeuGaussSeidel called ``sweeps`` times."""
+        pr, dtp = _ptr(res)
+        pb, _ = _ptr(b)
+        fn = getattr(lib(), "im3d_poisson_sweeps_" + _suffix(dtp))
+        self._check(fn(self._h, pr, pb, *map(C.c_int, res.shape), *map(C.c_double, h),
+                       C.c_double(dt), C.c_double(bc), C.c_int(bc_type), C.c_int(order),
+                       C.c_int(sweeps)))
+        return res
+
+    def poisson_solve(self, u, b, dt=1.0, bc=0.0, bc_type=BC_DIR, tol=1e-6, max_sweeps=1000,
+                      check_every=2, omega=1.0, h=(1.0, 1.0, 1.0)):
+        """In place on ``u``; returns (sweeps, relative residual, converged)."""
+        pu, dtp = _ptr(u)
+        pb, _ = _ptr(b)
+        sw = C.c_int(0)
+        rel = C.c_double(0)
+        fn = getattr(lib(), "im3d_poisson_solve_" + _suffix(dtp))
+        st = self._check(fn(self._h, pu, pb, *map(C.c_int, u.shape), *map(C.c_double, h),
+                            C.c_double(dt), C.c_double(bc), C.c_int(bc_type), C.c_double(tol),
+                            C.c_int(max_sweeps), C.c_int(check_every), C.c_double(omega),
+                            C.byref(sw), C.byref(rel)), allow=(ERR_NOT_CONVERGED,))
+        return int(sw.value), float(rel.value), st == OK
+
+    def rsfe_apply(self, myim, init=None, params: RsfeParams | None = None, h=(1.0, 1.0, 1.0),
+                   want_u=False, want_f=False, phi_out=None):
+        """segm::rsfe_splitbregman<T>::apply; returns dict(phi, u, f1, f2, stats)."""
+        p = params if params is not None else default_params()
+        pm, dt = _ptr(myim)
+        pi, _ = _ptr(init)
+        phi = _empty_like(myim) if phi_out is None else phi_out
+        u = _empty_like(myim) if want_u else None
+        f1 = _empty_like(myim) if want_f else None
+        f2 = _empty_like(myim) if want_f else None
+        st = RsfeStats()
+        fn = getattr(lib(), "im3d_rsfe_apply_" + _suffix(dt))
+        self._check(fn(self._h, pm, pi, *map(C.c_int, myim.shape), *map(C.c_double, h),
+                       C.byref(p), _ptr(phi)[0], _ptr(u)[0], _ptr(f1)[0], _ptr(f2)[0],
+                       C.byref(st)))
+        return dict(phi=phi, u=u, f1=f1, f2=f2, stats=st.as_dict())

@@ -1,0 +1,1035 @@
+// im3d_b200.cu -- host side of the sm_100a backend: context, device buffers, the
+// iteration of segm::rsfe_splitbregman<T>::apply, and the C ABI of include/im3d_b200.h.
+//
+// No CPU fallback: every numerical step below is a kernel of kernels.cuh. The host
+// only validates arguments, stages host buffers and steers the loop.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/im3d_b200.h"
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace im3d;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct im3d_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    std::unordered_map<std::string, DevBuf> bufs;
+    Ctrl* ctrl_d = nullptr;
+    Ctrl* ctrl_h = nullptr;  // pinned
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+#define IM3D_CUDA(ctx, call)                                                                  \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e_);                  \
+            return e_ == cudaErrorMemoryAllocation ? IM3D_ERR_OOM : IM3D_ERR_CUDA;             \
+        }                                                                                     \
+    } while (0)
+
+#define IM3D_TRY(...)                   \
+    do {                                \
+        int s_ = (__VA_ARGS__);         \
+        if (s_ != IM3D_OK) return s_;   \
+    } while (0)
+
+int fail(im3d_ctx* ctx, int code, const std::string& msg)
+{
+    ctx->err = msg;
+    return code;
+}
+
+int check_launch(im3d_ctx* ctx, const char* what)
+{
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("launch of ") + what + ": " + cudaGetErrorString(e);
+        return IM3D_ERR_CUDA;
+    }
+    return IM3D_OK;
+}
+
+// Device buffer of at least `bytes` under `name`, reused across calls.
+int buf(im3d_ctx* ctx, const char* name, size_t bytes, void** out, bool zero = false)
+{
+    DevBuf& b = ctx->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+        cudaError_t e = cudaMalloc(&b.p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ctx->err = std::string("cudaMalloc(") + name + ", " + std::to_string(bytes) +
+                       " bytes): " + cudaGetErrorString(e);
+            return IM3D_ERR_OOM;
+        }
+        b.bytes = bytes;
+    }
+    if (zero) IM3D_CUDA(ctx, cudaMemsetAsync(b.p, 0, bytes, ctx->stream));
+    *out = b.p;
+    return IM3D_OK;
+}
+
+template <typename T>
+int tbuf(im3d_ctx* ctx, const char* name, size_t count, T** out, bool zero = false)
+{
+    void* p = nullptr;
+    IM3D_TRY(buf(ctx, name, count * sizeof(T) + 256, &p, zero));
+    *out = static_cast<T*>(p);
+    return IM3D_OK;
+}
+
+bool is_device_ptr(const void* p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Input: a device pointer is used in place; a host pointer is copied to `slot`.
+template <typename T>
+int dev_in(im3d_ctx* ctx, const T* p, size_t count, const char* slot, const T** out)
+{
+    if (is_device_ptr(p)) {
+        *out = p;
+        return IM3D_OK;
+    }
+    T* d = nullptr;
+    IM3D_TRY(tbuf<T>(ctx, slot, count, &d));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(d, p, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    *out = d;
+    return IM3D_OK;
+}
+
+// Output staging: a device pointer is written directly; a host one goes through
+// `slot` and is copied back by out_finish.
+template <typename T>
+int dev_out(im3d_ctx* ctx, T* p, size_t count, const char* slot, T** out)
+{
+    if (!p) {
+        *out = nullptr;
+        return IM3D_OK;
+    }
+    if (is_device_ptr(p)) {
+        *out = p;
+        return IM3D_OK;
+    }
+    return tbuf<T>(ctx, slot, count, out);
+}
+
+template <typename T>
+int out_finish(im3d_ctx* ctx, T* user, const T* dev, size_t count)
+{
+    if (!user || user == dev) return IM3D_OK;
+    IM3D_CUDA(ctx, cudaMemcpyAsync(user, dev, count * sizeof(T), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    return IM3D_OK;
+}
+
+int sync(im3d_ctx* ctx)
+{
+    IM3D_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return IM3D_OK;
+}
+
+int check_dims(im3d_ctx* ctx, int nx, int ny, int nz, double hx, double hy, double hz)
+{
+    if (nx <= 0 || ny <= 0 || nz <= 0)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "dimensions must be positive");
+    if (nz == 1)
+        return fail(ctx, IM3D_ERR_UNSUPPORTED, "2-D volumes (nz == 1) are not supported by the "
+                                               "GPU backend");
+    if (nx < 3 || ny < 3 || nz < 3)
+        return fail(ctx, IM3D_ERR_UNSUPPORTED, "every dimension must be at least 3 (the "
+                                               "one-sided stencils read 3 points)");
+    if (!(hx > 0) || !(hy > 0) || !(hz > 0))
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "spacings must be positive");
+    if ((long long)nx * ny > 0x7fffffffLL || nx > 65535 || ny > 65535)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "volume too large for the launch geometry");
+    return IM3D_OK;
+}
+
+dim3 grid_vol(const Dims& d, dim3 blk) { return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, d.nx); }
+dim3 grid_pk(const Dims& d, dim3 blk) { return dim3((d.hz() + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, d.nx); }
+
+const dim3 kBlkVol(32, 8, 1);
+
+int flat_grid(long long n)
+{
+    long long b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// ------------------------------------------------------------- Gaussian taps
+// One axis of conv::filtering<T>::build_gaussian_filter (convolution_imp.hxx:22-80):
+// Nh = ceil(2 radius sigma / h), made odd; g[t] = exp(-(t-S)^2 h^2 / (2 sigma^2)).
+// The 3-D kernel normalised by its L1 norm is the product of these normalised 1-D
+// kernels, so each axis is normalised to unit sum.
+int gauss_taps_host(double sigma, double radius, double h, std::vector<double>& w)
+{
+    int nh = (int)std::ceil(2 * radius * sigma / h);
+    if (nh % 2 == 0) nh++;
+    if (nh > NH_MAX) return -1;
+    int S = nh / 2;
+    w.assign(nh, 0.0);
+    double s = 0;
+    for (int t = 0; t < nh; ++t) {
+        double dd = (double)(t - S);
+        w[t] = std::exp(-dd * dd * h * h / (2 * sigma * sigma));
+        s += w[t];
+    }
+    for (int t = 0; t < nh; ++t) w[t] /= s;
+    return nh;
+}
+
+template <typename T>
+struct Taps {
+    const T* w[3];
+    int nh[3];
+};
+
+template <typename T>
+int upload_taps(im3d_ctx* ctx, const char* slot, double sigma, double radius, double hx, double hy,
+                double hz, int pixel_approach, Taps<T>* out)
+{
+    if (!(sigma > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "sigma must be greater than zero");
+    if (!(radius > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "radius must be greater than zero");
+    const double hs[3] = {pixel_approach ? 1. : hx, pixel_approach ? 1. : hy,
+                          pixel_approach ? 1. : hz};
+    std::vector<T> host(3 * NH_MAX, T(0));
+    int nh[3];
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> w;
+        nh[a] = gauss_taps_host(sigma, radius, hs[a], w);
+        if (nh[a] < 0)
+            return fail(ctx, IM3D_ERR_UNSUPPORTED,
+                        "Gaussian support exceeds " + std::to_string(NH_MAX) +
+                            " taps (sigma*radius/h too large)");
+        for (int t = 0; t < nh[a]; ++t) host[a * NH_MAX + t] = (T)w[t];
+    }
+    T* d = nullptr;
+    IM3D_TRY(tbuf<T>(ctx, slot, 3 * NH_MAX, &d));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(d, host.data(), 3 * NH_MAX * sizeof(T), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    // the host vector must outlive the async copy
+    IM3D_TRY(sync(ctx));
+    for (int a = 0; a < 3; ++a) {
+        out->w[a] = d + a * NH_MAX;
+        out->nh[a] = nh[a];
+    }
+    return IM3D_OK;
+}
+
+// --------------------------------------------------------- convolution passes
+constexpr int TK = 128, RK = 2;
+constexpr int TW = 32, TY = 8;
+template <typename T> struct TileA { static constexpr int v = 64; };
+template <> struct TileA<double> { static constexpr int v = 32; };
+
+template <typename K>
+int set_smem(im3d_ctx* ctx, K kernel, size_t bytes)
+{
+    if (bytes > 48 * 1024)
+        IM3D_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)bytes));
+    return IM3D_OK;
+}
+
+template <typename T, int N, class Ld, class St>
+int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
+{
+    const int S = nh / 2;
+    size_t smem = (size_t)RK * (TK + 2 * S) * sizeof(Vec<T, N>) + nh * sizeof(T) + 16;
+    auto kern = conv_k_kernel<T, N, TK, RK, Ld, St>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    long long rows = (long long)d.nx * d.ny;
+    dim3 grid((unsigned)((rows + RK - 1) / RK), (d.nz + TK - 1) / TK);
+    kern<<<grid, dim3(TK, RK), smem, ctx->stream>>>(ld, st, d, w, nh);
+    return check_launch(ctx, "conv_k");
+}
+
+template <typename T, int N, int AXIS, class Ld, class St>
+int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
+{
+    constexpr int TA = TileA<T>::v;
+    const int S = nh / 2;
+    size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<T, N>) + nh * sizeof(T) + 16;
+    auto kern = conv_s_kernel<T, N, AXIS, TW, TY, TA, Ld, St>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    const int len = AXIS == 0 ? d.nx : d.ny;
+    const int other = AXIS == 0 ? d.ny : d.nx;
+    dim3 grid((d.nz + TW - 1) / TW, (len + TA - 1) / TA, other);
+    kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w, nh);
+    return check_launch(ctx, AXIS == 0 ? "conv_s(i)" : "conv_s(j)");
+}
+
+// Scalar Gaussian filter: in -> out through the three passes (tmp1, tmp2 scratch).
+template <typename T, class Ld>
+int gauss_scalar(im3d_ctx* ctx, Ld ld, T* out, const Dims& d, const Taps<T>& tp)
+{
+    Vec<T, 1>* t1 = nullptr;
+    Vec<T, 1>* t2 = nullptr;
+    IM3D_TRY(tbuf<Vec<T, 1>>(ctx, "gs_tmp1", d.n(), &t1));
+    IM3D_TRY(tbuf<Vec<T, 1>>(ctx, "gs_tmp2", d.n(), &t2));
+    IM3D_TRY((pass_k<T, 1>(ctx, ld, StVec<T, 1>{t1, d}, d, tp.w[2], tp.nh[2])));
+    IM3D_TRY((pass_s<T, 1, 1>(ctx, LdVec<T, 1>{t1, d}, StVec<T, 1>{t2, d}, d, tp.w[1], tp.nh[1])));
+    IM3D_TRY((pass_s<T, 1, 0>(ctx, LdVec<T, 1>{t2, d}, StScalar<T>{out, d}, d, tp.w[0], tp.nh[0])));
+    return IM3D_OK;
+}
+
+// -------------------------------------------------------------- Gauss-Seidel
+template <typename T>
+GsCoef<T> make_coef(double hx, double hy, double hz, double dt, double bc, int neu)
+{
+    GsCoef<T> c;
+    c.hx = hx; c.hy = hy; c.hz = hz; c.dt = dt;
+    c.ihx2 = (T)(1.0 / (hx * hx));
+    c.ihy2 = (T)(1.0 / (hy * hy));
+    c.ihz2 = (T)(1.0 / (hz * hz));
+    c.idt = (T)(1.0 / dt);
+    for (int m = 0; m < 8; ++m) {
+        // poisson_imp.hxx:115-139 / :398: htilde = 1/(1/dt + c_x/hx^2 + c_y/hy^2 + c_z/hz^2)
+        double cx = (m & 1) ? 2. : 1., cy = (m & 2) ? 2. : 1., cz = (m & 4) ? 2. : 1.;
+        double ht = 1. / dt + cx / (hx * hx) + cy / (hy * hy) + cz / (hz * hz);
+        c.htilde[m] = (T)(1. / ht);
+    }
+    // oblique normals of NeuGaussSeidel (poisson_imp.hxx:155-159): 1, 1/sqrt2, 1/sqrt3
+    const T tb = (T)bc;
+    T ne = T(1); ne /= (T)std::sqrt(2.);
+    T na = T(1); na /= (T)std::sqrt(3.);
+    c.bcn[0] = tb; c.bcn[1] = tb; c.bcn[2] = ne * tb; c.bcn[3] = na * tb;
+    for (int q = 0; q < 4; ++q) c.bcnd[q] = (double)c.bcn[q];
+    c.bc = tb;
+    c.neu = neu;
+    return c;
+}
+
+// One lexicographic sweep, reference order, natural layout, in place.
+template <typename T>
+int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c)
+{
+    if (!c.neu) {
+        dir_faces_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(r, d, c.bc);
+        IM3D_TRY(check_launch(ctx, "dir_faces"));
+    }
+    const int lo = c.neu ? 0 : 1;
+    const int hix = d.nx - lo, hiy = d.ny - lo, hiz = d.nz - lo;
+    if (hix <= lo || hiy <= lo || hiz <= lo) return IM3D_OK;
+    const dim3 blk(32, 4);
+    for (int s = 3 * lo; s <= (hix - 1) + (hiy - 1) + (hiz - 1); ++s) {
+        const int i0 = std::max(lo, s - (hiy - 1) - (hiz - 1));
+        const int i1 = std::min(hix - 1, s - 2 * lo);
+        if (i0 > i1) continue;
+        const int j0 = std::max(lo, s - i1 - (hiz - 1));
+        const int j1 = std::min(hiy - 1, s - i0 - lo);
+        if (j0 > j1) continue;
+        dim3 grid((j1 - j0 + 1 + blk.x - 1) / blk.x, (i1 - i0 + 1 + blk.y - 1) / blk.y);
+        lex_plane_kernel<T><<<grid, blk, 0, ctx->stream>>>(r, b, d, c, s, lo, i0, j0);
+        IM3D_TRY(check_launch(ctx, "lex_plane"));
+    }
+    return IM3D_OK;
+}
+
+template <typename T>
+int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, int use_self,
+             double omega)
+{
+    for (int color = 0; color < 2; ++color) {
+        rb_half_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(U, B, d, c, color,
+                                                                          use_self, (T)omega);
+        IM3D_TRY(check_launch(ctx, "rb_half"));
+    }
+    return IM3D_OK;
+}
+
+int zero_ctrl(im3d_ctx* ctx)
+{
+    IM3D_CUDA(ctx, cudaMemsetAsync(ctx->ctrl_d, 0, sizeof(Ctrl), ctx->stream));
+    return IM3D_OK;
+}
+
+int read_ctrl(im3d_ctx* ctx)
+{
+    IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->ctrl_h, ctx->ctrl_d, sizeof(Ctrl), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    return sync(ctx);
+}
+
+// Red-black solve on the packed layout (U holds u_in on entry, B = b_eff packed).
+// Residual every check_every sweeps; sum b_eff^2 is taken on the first check.
+template <typename T>
+int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, double tol,
+             int max_sweeps, int check_every, double omega, int* sweeps, double* rel, bool* conv)
+{
+    if (check_every < 1) check_every = 1;
+    if (max_sweeps < 1) max_sweeps = 1;
+    double beff2 = -1;
+    int s = 0;
+    *conv = false;
+    *rel = -1;
+    while (s < max_sweeps) {
+        IM3D_TRY(rb_sweep(ctx, U, B, d, c, 0, omega));
+        ++s;
+        if (s % check_every == 0 || s == max_sweeps) {
+            IM3D_TRY(zero_ctrl(ctx));
+            rb_residual_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+                U, B, d, c, ctx->ctrl_d->sum, beff2 < 0 ? 1 : 0);
+            IM3D_TRY(check_launch(ctx, "rb_residual"));
+            IM3D_TRY(read_ctrl(ctx));
+            if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
+            const double rr = ctx->ctrl_h->sum[SUM_RES2];
+            *rel = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
+            if (*rel <= tol) {
+                *conv = true;
+                break;
+            }
+        }
+    }
+    *sweeps = s;
+    return IM3D_OK;
+}
+
+// --------------------------------------------------------------- the loop
+template <typename T>
+struct Outs {
+    T* phi;
+    T* u;
+    T* f1;
+    T* f2;
+};
+
+template <typename T>
+int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, int ny, int nz,
+               double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
+               T* f1_user, T* f2_user, im3d_rsfe_stats* stats)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!p) return fail(ctx, IM3D_ERR_INVALID_ARG, "params must not be NULL");
+    if (!myim_user || !phi_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "myim and phi_out are required");
+    // the setters' checks (rsfe_splitbregman_imp.hxx:806-1440)
+    if (!(p->sigma > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_sigma: sigma must be greater than zero");
+    if (!(p->lamda > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_lamda: lamda must be greater than zero");
+    if (!(p->lamda1 > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_lamda1: lamda1 must be greater than zero");
+    if (!(p->lamda2 > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_lamda2: lamda2 must be greater than zero");
+    if (!(p->dt > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_dt: dt must be greater than zero");
+    if (!(p->epsilon > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_epsilon: epsilon must be greater than zero");
+    if (!(p->nu >= 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_nu: nu must be non negative");
+    if (!(p->beta >= 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_beta: beta must be non negative");
+    if (!(p->tol >= 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_tol: tol must be greater than zero");
+    if (!(p->ls_tol >= 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_tol: tol must be positive");
+    if (p->ls_steps <= 0) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_ls_steps: ls_steps must be greater than 0");
+    if (!(p->edge_detector_sigma >= 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_edge_detector_sigma: edge_detector_sigma must be greater than zero");
+    if (p->bc != IM3D_BC_DEFAULT && p->bc != IM3D_BC_NEU && p->bc != IM3D_BC_DIR)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_bc: specify a proper bc_type condition");
+    if (!(p->b0 > p->a0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "b0 has to be greater than a0");
+    if (p->gs_rel_res_tol > 0 && !(p->omega > 0 && p->omega < 2))
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "omega must lie in (0, 2)");
+
+    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    const Dims d{nx, ny, nz};
+    const long long n = d.n();
+    const long long npk2 = 2 * d.npk();
+    const bool solve = p->gs_rel_res_tol > 0;
+    const bool lex = !solve && p->sweep == IM3D_SWEEP_LEXICOGRAPHIC;
+    const bool neu = p->bc == IM3D_BC_NEU;
+    // chosen_bc (rsfe_splitbregman_imp.hxx:1735-1743): NEU (also the ctor default) -> 0
+    const double chosen_bc = p->bc == IM3D_BC_DIR ? p->a0 : 0.0;
+    const T a0 = (T)p->a0, b0 = (T)p->b0;
+
+    const T* u0 = nullptr;
+    const T* init = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, myim_user, n, "in_myim", &u0));
+    if (init_user) IM3D_TRY(dev_in<T>(ctx, init_user, n, "in_init", &init));
+
+    T *phiA, *phiB, *g, *divdb, *b3, *dmb, *kones = nullptr, *rhs = nullptr, *upk = nullptr,
+      *bpk = nullptr, *prev = nullptr;
+    Vec<T, 4>*W1, *W2;
+    Vec<T, 2>*P1, *P2;
+    IM3D_TRY(tbuf<T>(ctx, "phiA", n, &phiA));
+    IM3D_TRY(tbuf<T>(ctx, "phiB", n, &phiB));
+    IM3D_TRY(tbuf<T>(ctx, "g", n, &g));
+    IM3D_TRY(tbuf<T>(ctx, "divdb", n, &divdb, true));
+    IM3D_TRY(tbuf<T>(ctx, "b3", 3 * n, &b3, true));
+    IM3D_TRY(tbuf<T>(ctx, "dmb", 3 * n, &dmb));
+    IM3D_TRY(tbuf<Vec<T, 4>>(ctx, "W1", n, &W1));
+    IM3D_TRY(tbuf<Vec<T, 4>>(ctx, "W2", n, &W2));
+    IM3D_TRY(tbuf<Vec<T, 2>>(ctx, "P1", n, &P1));
+    IM3D_TRY(tbuf<Vec<T, 2>>(ctx, "P2", n, &P2));
+    if (p->lamda1 != p->lamda2) IM3D_TRY(tbuf<T>(ctx, "kones", n, &kones));
+    if (lex) IM3D_TRY(tbuf<T>(ctx, "rhs", n, &rhs));
+    else {
+        IM3D_TRY(tbuf<T>(ctx, "upk", npk2, &upk, true));
+        IM3D_TRY(tbuf<T>(ctx, "bpk", npk2, &bpk, true));
+    }
+    if (p->ls_tol != 0 && !solve) IM3D_TRY(tbuf<T>(ctx, "prev", lex ? n : npk2, &prev, true));
+    T *u_d = nullptr, *f1_d = nullptr, *f2_d = nullptr;
+    IM3D_TRY(dev_out<T>(ctx, u_user, n, "out_u", &u_d));
+    IM3D_TRY(dev_out<T>(ctx, f1_user, n, "out_f1", &f1_d));
+    IM3D_TRY(dev_out<T>(ctx, f2_user, n, "out_f2", &f2_d));
+    if (f1_d && !f2_d) IM3D_TRY(tbuf<T>(ctx, "out_f2", n, &f2_d));
+    if (f2_d && !f1_d) IM3D_TRY(tbuf<T>(ctx, "out_f1", n, &f1_d));
+
+    // initial level set (rsfe_splitbregman_imp.hxx:99-170 / :48-95), then
+    // change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636)
+    if (init) {
+        IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, init, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        const int ix = (int)(nx * 0.33), iy = (int)(ny * 0.33), iz = (int)(nz * 0.33);
+        const int fx = (int)(nx * (1 - 0.33)), fy = (int)(ny * (1 - 0.33)), fz = (int)(nz * (1 - 0.33));
+        cube_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(phiA, d, ix, iy, iz, fx,
+                                                                           fy, fz, a0, b0);
+        IM3D_TRY(check_launch(ctx, "cube"));
+    }
+    {
+        IM3D_TRY(zero_ctrl(ctx));
+        minmax_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(phiA, n, ctx->ctrl_d->umax);
+        IM3D_TRY(check_launch(ctx, "minmax"));
+        IM3D_TRY(read_ctrl(ctx));
+        auto key_to_double = [](unsigned long long k) {
+            unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+            double v;
+            std::memcpy(&v, &b, sizeof v);
+            return v;
+        };
+        const T mx = (T)key_to_double(ctx->ctrl_h->umax[0]);
+        const T mn = (T)(-key_to_double(ctx->ctrl_h->umax[1]));
+        const T shifted_max = mx - mn;
+        const T s = shifted_max / (T)(b0 - a0);
+        affine_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(phiA, n, mn, s, a0);
+        IM3D_TRY(check_launch(ctx, "affine"));
+    }
+
+    // filters, kones (only used when lamda1 != lamda2), edge detector
+    Taps<T> tp;
+    IM3D_TRY(upload_taps<T>(ctx, "taps", p->sigma, 3.0, hx, hy, hz, p->gaussian_pixel_approach, &tp));
+    if (kones) IM3D_TRY(gauss_scalar<T>(ctx, LdOne<T>{}, kones, d, tp));
+    {
+        const T* src = u0;
+        if (p->edge_detector_sigma != 0) {
+            Taps<T> te;
+            IM3D_TRY(upload_taps<T>(ctx, "taps_eds", p->edge_detector_sigma, 3.0, hx, hy, hz,
+                                    p->gaussian_pixel_approach, &te));
+            T* blurred = nullptr;
+            IM3D_TRY(tbuf<T>(ctx, "eds_blur", n, &blurred));
+            IM3D_TRY(gauss_scalar<T>(ctx, LdScalar<T>{u0, d}, blurred, d, te));
+            src = blurred;
+        }
+        edge_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+            src, g, d, hx, hy, hz, (T)p->beta, (T)p->lamda, (T)p->nu);
+        IM3D_TRY(check_launch(ctx, "edge"));
+    }
+    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+
+    const GsCoef<T> coef = make_coef<T>(hx, hy, hz, p->dt, chosen_bc, neu ? 1 : 0);
+    const T center = (T)((p->a0 + p->b0) / 2.);
+    const T inv_eps = (T)(1.0 / p->epsilon);
+    const double hhh = hx * hy * hz;
+    double tollerance = 1000;
+    int init_variables = p->init_variables;
+    long long total_sweeps = 0;
+    int last_sweeps = 0, not_conv = 0, t;
+    double last_rel = -1, last_ls_err = -1;
+    T* phi = phiA;   // current level set (natural)
+    T* other = phiB;
+
+    for (t = 1; tollerance > p->tol && t <= p->maxiter; ++t) {
+        // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
+        IM3D_TRY((pass_k<T, 4>(ctx, LdHeaviside<T>{phi, u0, d, center, inv_eps}, StVec<T, 4>{W1, d},
+                               d, tp.w[2], tp.nh[2])));
+        IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1])));
+        {
+            constexpr int TA = TileA<T>::v;
+            const int S = tp.nh[0] / 2;
+            size_t smem = (size_t)(TA + 4 * S) * TW * sizeof(Vec<T, 4>) +
+                          (size_t)(TA + 2 * S) * TW * sizeof(Vec<T, 2>) + tp.nh[0] * sizeof(T) + 16;
+            auto kern = conv_i_fit_kernel<T, TW, TY, TA>;
+            IM3D_TRY(set_smem(ctx, kern, smem));
+            dim3 grid((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny);
+            kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(W2, P1, f1_d, f2_d, d, tp.w[0],
+                                                           tp.nh[0], (T)p->lamda1, (T)p->lamda2);
+            IM3D_TRY(check_launch(ctx, "conv_i_fit"));
+        }
+        IM3D_TRY((pass_s<T, 2, 1>(ctx, LdVec<T, 2>{P1, d}, StVec<T, 2>{P2, d}, d, tp.w[1], tp.nh[1])));
+        {
+            StRhs<T> st;
+            st.u0 = u0; st.kones = kones; st.divdb = divdb; st.phi = phi;
+            st.out = lex ? rhs : bpk;
+            st.upk = upk;
+            st.beff2 = nullptr;
+            st.d = d;
+            st.l12 = (T)(p->lamda1 - p->lamda2);
+            st.lamda = (T)p->lamda;
+            st.inv_dt = (T)(1.0 / p->dt);
+            st.bc = (T)chosen_bc;
+            st.mode = lex ? 0 : (solve ? 2 : 1);
+            st.dirichlet = neu ? 0 : 1;
+            IM3D_TRY((pass_k<T, 2>(ctx, LdVec<T, 2>{P2, d}, st, d, tp.w[2], tp.nh[2])));
+        }
+
+        // the Poisson step (rsfe_splitbregman_imp.hxx:1768-1785)
+        T* uu;  // where the solved u lives (natural `phi` for lex, packed otherwise)
+        if (solve) {
+            int sw = 0;
+            double rel = -1;
+            bool conv = false;
+            IM3D_TRY(rb_solve<T>(ctx, upk, bpk, d, coef, p->gs_rel_res_tol, p->gs_max_sweeps,
+                                 p->gs_check_every, p->omega, &sw, &rel, &conv));
+            if (!conv) not_conv++;
+            total_sweeps += sw;
+            last_sweeps = sw;
+            last_rel = rel;
+            uu = upk;
+        } else {
+            if (lex) IM3D_CUDA(ctx, cudaMemcpyAsync(other, phi, n * sizeof(T), cudaMemcpyDeviceToDevice,
+                                                    ctx->stream));
+            T* work = lex ? phi : upk;
+            const long long cnt = lex ? n : npk2;
+            double ls_err = p->ls_tol ? 1000. : -1.;
+            int s;
+            for (s = 0; s < p->ls_steps || ls_err > p->ls_tol; ++s) {
+                if (s >= 100000) {
+                    not_conv++;
+                    break;
+                }
+                if (p->ls_tol != 0)
+                    IM3D_CUDA(ctx, cudaMemcpyAsync(prev, work, cnt * sizeof(T), cudaMemcpyDeviceToDevice,
+                                                   ctx->stream));
+                if (lex) IM3D_TRY(lex_sweep<T>(ctx, phi, rhs, d, coef));
+                else IM3D_TRY(rb_sweep<T>(ctx, upk, bpk, d, coef, 1, 1.0));
+                if (p->ls_tol != 0 && s >= p->ls_steps - 1) {
+                    IM3D_TRY(zero_ctrl(ctx));
+                    diff_sums_kernel<T><<<flat_grid(cnt), 256, 0, ctx->stream>>>(work, prev, cnt,
+                                                                               ctx->ctrl_d->sum);
+                    IM3D_TRY(check_launch(ctx, "diff_sums"));
+                    IM3D_TRY(read_ctrl(ctx));
+                    ls_err = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_A]) /
+                             std::sqrt(hhh * ctx->ctrl_h->sum[SUM_B]);
+                }
+            }
+            total_sweeps += s;
+            last_sweeps = s;
+            last_ls_err = ls_err;
+            uu = lex ? phi : upk;
+        }
+
+        // clamp, tolerance, Bregman update, div(d - b)
+        IM3D_TRY(zero_ctrl(ctx));
+        T* phi_new = lex ? other : phi;  // lex: `other` holds phiold and receives the clamp
+        const int bregman = init_variables ? 0 : 1;
+        if (lex)
+            post_solve_kernel<T, false><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+                uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
+        else
+            post_solve_kernel<T, true><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+                uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
+        IM3D_TRY(check_launch(ctx, "post_solve"));
+        if (init_variables) {
+            IM3D_CUDA(ctx, cudaMemsetAsync(divdb, 0, n * sizeof(T), ctx->stream));
+            IM3D_CUDA(ctx, cudaMemsetAsync(b3, 0, 3 * n * sizeof(T), ctx->stream));
+            init_variables = 0;
+        } else {
+            div_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(dmb, divdb, d, hx, hy, hz);
+            IM3D_TRY(check_launch(ctx, "div"));
+        }
+        IM3D_TRY(read_ctrl(ctx));
+        tollerance = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_DPHI2]) /
+                     std::sqrt(hhh * ctx->ctrl_h->sum[SUM_PHIOLD2]);
+        if (lex) std::swap(phi, other);
+    }
+    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+
+    // outputs
+    if (is_device_ptr(phi_user)) {
+        IM3D_CUDA(ctx, cudaMemcpyAsync(phi_user, phi, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        IM3D_CUDA(ctx, cudaMemcpyAsync(phi_user, phi, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    IM3D_TRY(out_finish<T>(ctx, u_user, u_d, n));
+    IM3D_TRY(out_finish<T>(ctx, f1_user, f1_d, n));
+    IM3D_TRY(out_finish<T>(ctx, f2_user, f2_d, n));
+    IM3D_TRY(sync(ctx));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->iterations = t - 1;
+        stats->last_tol = tollerance;
+        stats->total_sweeps = total_sweeps;
+        stats->last_sweeps = last_sweeps;
+        stats->last_rel_res = last_rel;
+        stats->last_ls_err = last_ls_err;
+        stats->not_converged = not_conv;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+        stats->setup_ms = ms;
+        cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+        stats->loop_ms = ms;
+    }
+    return IM3D_OK;
+}
+
+// ------------------------------------------------------ standalone operators
+template <typename T>
+int gauss_filter(im3d_ctx* ctx, const T* in_user, T* out_user, int nx, int ny, int nz, double hx,
+                 double hy, double hz, double sigma, double radius, int pixel_approach)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!in_user || !out_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    const Dims d{nx, ny, nz};
+    const T* in = nullptr;
+    T* out = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, in_user, d.n(), "in_a", &in));
+    IM3D_TRY(dev_out<T>(ctx, out_user, d.n(), "out_a", &out));
+    Taps<T> tp;
+    IM3D_TRY(upload_taps<T>(ctx, "taps_op", sigma, radius, hx, hy, hz, pixel_approach, &tp));
+    IM3D_TRY(gauss_scalar<T>(ctx, LdScalar<T>{in, d}, out, d, tp));
+    IM3D_TRY(out_finish<T>(ctx, out_user, out, d.n()));
+    return sync(ctx);
+}
+
+template <typename T>
+int grad_op(im3d_ctx* ctx, const T* in_user, T* out_user, int nx, int ny, int nz, double hx,
+            double hy, double hz)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!in_user || !out_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    const Dims d{nx, ny, nz};
+    const T* in = nullptr;
+    T* out = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, in_user, d.n(), "in_a", &in));
+    IM3D_TRY(dev_out<T>(ctx, out_user, 3 * d.n(), "out_a", &out));
+    grad_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(in, out, d, hx, hy, hz);
+    IM3D_TRY(check_launch(ctx, "grad"));
+    IM3D_TRY(out_finish<T>(ctx, out_user, out, 3 * d.n()));
+    return sync(ctx);
+}
+
+template <typename T>
+int div_op(im3d_ctx* ctx, const T* in_user, T* out_user, int nx, int ny, int nz, double hx,
+           double hy, double hz)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!in_user || !out_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    const Dims d{nx, ny, nz};
+    const T* in = nullptr;
+    T* out = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, in_user, 3 * d.n(), "in_a", &in));
+    IM3D_TRY(dev_out<T>(ctx, out_user, d.n(), "out_a", &out));
+    div_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(in, out, d, hx, hy, hz);
+    IM3D_TRY(check_launch(ctx, "div"));
+    IM3D_TRY(out_finish<T>(ctx, out_user, out, d.n()));
+    return sync(ctx);
+}
+
+template <typename T>
+int poisson_sweeps(im3d_ctx* ctx, T* res_user, const T* b_user, int nx, int ny, int nz, double hx,
+                   double hy, double hz, double dt, double bc, int bc_type, int order, int sweeps)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!res_user || !b_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    if (!(dt > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "dt must be greater than zero");
+    if (sweeps < 0) return fail(ctx, IM3D_ERR_INVALID_ARG, "sweeps must be non negative");
+    if (order != IM3D_SWEEP_LEXICOGRAPHIC && order != IM3D_SWEEP_REDBLACK)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown sweep order");
+    const Dims d{nx, ny, nz};
+    const long long n = d.n();
+    const GsCoef<T> c = make_coef<T>(hx, hy, hz, dt, bc, bc_type == IM3D_BC_NEU ? 1 : 0);
+    const T* b = nullptr;
+    T* r = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, b_user, n, "in_b", &b));
+    if (is_device_ptr(res_user)) r = res_user;
+    else {
+        IM3D_TRY(tbuf<T>(ctx, "io_res", n, &r));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(r, res_user, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (order == IM3D_SWEEP_LEXICOGRAPHIC) {
+        for (int s = 0; s < sweeps; ++s) IM3D_TRY(lex_sweep<T>(ctx, r, b, d, c));
+    } else if (sweeps > 0) {
+        // DirGaussSeidel assigns the boundary value before sweeping (poisson_imp.hxx:366-391)
+        if (!c.neu) {
+            dir_faces_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(r, d, c.bc);
+            IM3D_TRY(check_launch(ctx, "dir_faces"));
+        }
+        T *U, *B;
+        IM3D_TRY(tbuf<T>(ctx, "op_upk", 2 * d.npk(), &U, true));
+        IM3D_TRY(tbuf<T>(ctx, "op_bpk", 2 * d.npk(), &B, true));
+        pack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(r, U, d);
+        IM3D_TRY(check_launch(ctx, "pack"));
+        pack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(b, B, d);
+        IM3D_TRY(check_launch(ctx, "pack"));
+        for (int s = 0; s < sweeps; ++s) IM3D_TRY(rb_sweep<T>(ctx, U, B, d, c, 1, 1.0));
+        unpack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(U, r, d);
+        IM3D_TRY(check_launch(ctx, "unpack"));
+    }
+    if (r != res_user)
+        IM3D_CUDA(ctx, cudaMemcpyAsync(res_user, r, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    return sync(ctx);
+}
+
+template <typename T>
+int poisson_solve(im3d_ctx* ctx, T* u_user, const T* b_user, int nx, int ny, int nz, double hx,
+                  double hy, double hz, double dt, double bc, int bc_type, double tol,
+                  int max_sweeps, int check_every, double omega, int* sweeps_done, double* rel_res)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!u_user || !b_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    if (!(dt > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "dt must be greater than zero");
+    if (!(omega > 0 && omega < 2)) return fail(ctx, IM3D_ERR_INVALID_ARG, "omega must lie in (0, 2)");
+    const Dims d{nx, ny, nz};
+    const long long n = d.n();
+    const int neu = bc_type == IM3D_BC_NEU ? 1 : 0;
+    const GsCoef<T> c = make_coef<T>(hx, hy, hz, dt, bc, neu);
+    const T* b = nullptr;
+    T* r = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, b_user, n, "in_b", &b));
+    if (is_device_ptr(u_user)) r = u_user;
+    else {
+        IM3D_TRY(tbuf<T>(ctx, "io_res", n, &r));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(r, u_user, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    T *U, *B;
+    IM3D_TRY(tbuf<T>(ctx, "op_upk", 2 * d.npk(), &U, true));
+    IM3D_TRY(tbuf<T>(ctx, "op_bpk", 2 * d.npk(), &B, true));
+    pack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(r, U, d);
+    IM3D_TRY(check_launch(ctx, "pack"));
+    IM3D_TRY(zero_ctrl(ctx));
+    make_beff_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+        b, U, B, d, (T)(1.0 / dt), (T)bc, neu ? 0 : 1, ctx->ctrl_d->sum);
+    IM3D_TRY(check_launch(ctx, "make_beff"));
+    int sw = 0;
+    double rel = -1;
+    bool conv = false;
+    IM3D_TRY(rb_solve<T>(ctx, U, B, d, c, tol, max_sweeps, check_every, omega, &sw, &rel, &conv));
+    unpack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(U, r, d);
+    IM3D_TRY(check_launch(ctx, "unpack"));
+    if (r != u_user)
+        IM3D_CUDA(ctx, cudaMemcpyAsync(u_user, r, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    IM3D_TRY(sync(ctx));
+    if (sweeps_done) *sweeps_done = sw;
+    if (rel_res) *rel_res = rel;
+    if (!conv) return fail(ctx, IM3D_ERR_NOT_CONVERGED, "sweep cap reached before the tolerance");
+    return IM3D_OK;
+}
+
+int enter(im3d_ctx* ctx)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    ctx->err.clear();
+    IM3D_CUDA(ctx, cudaSetDevice(ctx->device));
+    return IM3D_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int im3d_ctx_create(int device, im3d_ctx** out)
+{
+    if (!out) return IM3D_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return IM3D_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return IM3D_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        cudaGetLastError();
+        return IM3D_ERR_NO_DEVICE;
+    }
+    im3d_ctx* ctx = new im3d_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->ctrl_d, sizeof(Ctrl)) != cudaSuccess ||
+        cudaMallocHost(&ctx->ctrl_h, sizeof(Ctrl)) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return IM3D_ERR_CUDA;
+    }
+    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return IM3D_OK;
+}
+
+int im3d_ctx_destroy(im3d_ctx* ctx)
+{
+    if (!ctx) return IM3D_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    if (ctx->ctrl_d) cudaFree(ctx->ctrl_d);
+    if (ctx->ctrl_h) cudaFreeHost(ctx->ctrl_h);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return IM3D_OK;
+}
+
+const char* im3d_ctx_last_error(const im3d_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+int im3d_ctx_set_stream(im3d_ctx* ctx, void* stream)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return IM3D_OK;
+}
+
+int64_t im3d_ctx_launch_count(const im3d_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void im3d_rsfe_params_default(im3d_rsfe_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    // rsfe_splitbregman_imp.hxx:25-41
+    p->tol = 1.e-5;
+    p->sigma = 3;
+    p->lamda = 5.e-2;
+    p->lamda1 = 1.e-5;
+    p->lamda2 = 1.e-5;
+    p->beta = 100.;
+    p->nu = 1.;
+    p->dt = 1;
+    p->epsilon = 1.e-3;
+    p->a0 = 0.;
+    p->b0 = 1.;
+    p->ls_tol = 0;
+    p->edge_detector_sigma = 0;
+    p->maxiter = 100;
+    p->ls_steps = 5;
+    p->bc = IM3D_BC_DEFAULT;
+    p->gaussian_pixel_approach = 0;
+    p->init_variables = 0;
+    // extensions
+    p->sweep = IM3D_SWEEP_LEXICOGRAPHIC;
+    p->gs_rel_res_tol = 0;
+    p->omega = 1.0;
+    p->gs_max_sweeps = 1000;
+    p->gs_check_every = 2;
+}
+
+#define IM3D_ENTRY(...)                \
+    do {                               \
+        int s_ = enter(ctx);           \
+        if (s_ != IM3D_OK) return s_;  \
+        return __VA_ARGS__;            \
+    } while (0)
+
+int im3d_gauss_filter_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
+                          double hx, double hy, double hz, double sigma, double radius,
+                          int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
+}
+
+int im3d_gauss_filter_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
+                          double hx, double hy, double hz, double sigma, double radius,
+                          int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<double>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
+}
+
+int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,
+                            double hx, double hy, double hz, double dt, double bc, int bc_type,
+                            int sweep_order, int sweeps)
+{
+    IM3D_ENTRY(poisson_sweeps<float>(ctx, res, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, sweep_order, sweeps));
+}
+
+int im3d_poisson_sweeps_f64(im3d_ctx* ctx, double* res, const double* b, int nx, int ny, int nz,
+                            double hx, double hy, double hz, double dt, double bc, int bc_type,
+                            int sweep_order, int sweeps)
+{
+    IM3D_ENTRY(poisson_sweeps<double>(ctx, res, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, sweep_order, sweeps));
+}
+
+int im3d_poisson_solve_f32(im3d_ctx* ctx, float* u, const float* b, int nx, int ny, int nz,
+                           double hx, double hy, double hz, double dt, double bc, int bc_type,
+                           double rel_res_tol, int max_sweeps, int check_every, double omega,
+                           int* sweeps_done, double* rel_res)
+{
+    IM3D_ENTRY(poisson_solve<float>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
+                                    max_sweeps, check_every, omega, sweeps_done, rel_res));
+}
+
+int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, int ny, int nz,
+                           double hx, double hy, double hz, double dt, double bc, int bc_type,
+                           double rel_res_tol, int max_sweeps, int check_every, double omega,
+                           int* sweeps_done, double* rel_res)
+{
+    IM3D_ENTRY(poisson_solve<double>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
+                                     max_sweeps, check_every, omega, sweeps_done, rel_res));
+}
+
+int im3d_grad_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz, double hx,
+                  double hy, double hz)
+{
+    IM3D_ENTRY(grad_op<float>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_grad_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
+                  double hy, double hz)
+{
+    IM3D_ENTRY(grad_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_div_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz, double hx,
+                 double hy, double hz)
+{
+    IM3D_ENTRY(div_op<float>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_div_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
+                 double hy, double hz)
+{
+    IM3D_ENTRY(div_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_rsfe_apply_f32(im3d_ctx* ctx, const float* myim, const float* init, int nx, int ny, int nz,
+                        double hx, double hy, double hz, const im3d_rsfe_params* p, float* phi_out,
+                        float* u_out, float* f1_out, float* f2_out, im3d_rsfe_stats* stats)
+{
+    IM3D_ENTRY(rsfe_apply<float>(ctx, myim, init, nx, ny, nz, hx, hy, hz, p, phi_out, u_out, f1_out,
+                                 f2_out, stats));
+}
+
+int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, int nx, int ny,
+                        int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
+                        double* phi_out, double* u_out, double* f1_out, double* f2_out,
+                        im3d_rsfe_stats* stats)
+{
+    IM3D_ENTRY(rsfe_apply<double>(ctx, myim, init, nx, ny, nz, hx, hy, hz, p, phi_out, u_out, f1_out,
+                                  f2_out, stats));
+}
+
+}  // extern "C"

@@ -1,24 +1,27 @@
 /*
  * fft_shim.cpp -- FP64 complex DFT behind the FFTW3 names declared in fftw3.h.
  *
- * TEST INFRASTRUCTURE ONLY (the CPU checker's build of the reference).
+ * TEST INFRASTRUCTURE ONLY (the CPU checker's build of the reference, which is also
+ * the timed CPU baseline; FFTW itself is not available on this machine).
  *
  * Written from the DFT definition and two published algorithms:
- *  - mixed-radix Cooley-Tukey (decimation in time, recursive, out of place) for
- *    lengths whose prime factors are all <= 7;
- *  - Bluestein's chirp-z identity jk = (j^2 + k^2 - (k-j)^2)/2 for every other
- *    length, turning a length-n DFT into a circular convolution of power-of-two
- *    length m >= 2n-1 (evaluated with the radix-2 path above).
+ *  - mixed-radix Cooley-Tukey, decimation in time, recursive and out of place, with
+ *    radices 4, 2, 3, 5, 7 (radix 2 and 4 butterflies written out);
+ *  - Bluestein's chirp-z identity jk = (j^2 + k^2 - (k-j)^2)/2 for the part of the
+ *    length with no factor <= 7, turning that DFT into a circular convolution of
+ *    power-of-two length m >= 2p-1 (e.g. 274 = 2 * 137: two length-137 Bluestein
+ *    transforms of size 512 under one radix-2 stage).
  * Twiddles are computed directly with cos/sin of an exactly reduced angle (no
  * recurrences), so the transform is accurate to a few ulp times log2(n).
- * A 3-D transform is three batches of 1-D transforms (axis 2 is contiguous),
- * parallel over lines with OpenMP, as FFTW's threaded planner would run it.
+ * A 3-D transform is three batches of 1-D transforms (axis 2 contiguous), parallel
+ * over lines with OpenMP, as FFTW's threaded planner would run it.
  */
 #include "fftw3.h"
 
 #include <cmath>
 #include <complex>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 #include <omp.h>
@@ -26,139 +29,143 @@
 namespace {
 
 typedef std::complex<double> cplx;
+const double kPi = 3.14159265358979323846264338327950288;
 
 struct Plan1D {
     int n = 0;
     int sign = -1;
-    bool bluestein = false;
-    std::vector<int> factors;  // Cooley-Tukey radices, product = n
+    std::vector<int> factors;  // small radices; their product times `large` is n
+    int large = 1;             // cofactor with no prime factor <= 7 (Bluestein)
     std::vector<cplx> tw;      // tw[e] = exp(sign*2*pi*i*e/n), e in [0, n)
-    // Bluestein state
+    // Bluestein of length `large` (pow2 size m)
     int m = 0;
-    std::vector<cplx> chirp;   // c[k] = exp(sign*i*pi*k^2/n)
-    std::vector<cplx> bhat;    // FFT_m of conj(chirp) arranged circularly
-    Plan1D* fwd_m = nullptr;   // length-m forward transform
-    Plan1D* bwd_m = nullptr;   // length-m backward transform
-
+    std::vector<cplx> chirp;   // exp(sign*i*pi*k^2/large)
+    std::vector<cplx> bhat;    // FFT_m of conj(chirp), circular
+    Plan1D* fwd_m = nullptr;
+    Plan1D* bwd_m = nullptr;
     ~Plan1D() { delete fwd_m; delete bwd_m; }
 };
 
-const double kPi = 3.14159265358979323846264338327950288;
-
-void exec_1d(const Plan1D* p, const cplx* in, cplx* out, cplx* scratch);
-
-bool factorize_small(int n, std::vector<int>& f)
-{
-    f.clear();
-    int r = n;
-    while (r % 4 == 0) { f.push_back(4); r /= 4; }
-    const int primes[] = {2, 3, 5, 7};
-    for (int p : primes)
-        while (r % p == 0) { f.push_back(p); r /= p; }
-    return r == 1;
-}
-
-Plan1D* make_plan(int n, int sign);
-
-void init_twiddles(Plan1D* p)
-{
-    p->tw.resize(p->n);
-    for (int e = 0; e < p->n; ++e) {
-        double ang = p->sign * 2.0 * kPi * (double)e / (double)p->n;
-        p->tw[e] = cplx(std::cos(ang), std::sin(ang));
-    }
-}
+void exec_1d(const Plan1D* p, const cplx* in, long stride, cplx* out, cplx* scratch);
 
 Plan1D* make_plan(int n, int sign)
 {
     Plan1D* p = new Plan1D();
     p->n = n;
     p->sign = sign;
-    if (n <= 1 || factorize_small(n, p->factors)) {
-        if (n <= 1) p->factors.clear();
-        init_twiddles(p);
-        return p;
+    int r = n;
+    while (r % 4 == 0) { p->factors.push_back(4); r /= 4; }
+    const int primes[] = {2, 3, 5, 7};
+    for (int q : primes)
+        while (r % q == 0) { p->factors.push_back(q); r /= q; }
+    p->large = r;
+    p->tw.resize(n);
+    for (int e = 0; e < n; ++e) {
+        double ang = sign * 2.0 * kPi * (double)e / (double)n;
+        p->tw[e] = cplx(std::cos(ang), std::sin(ang));
     }
-    // Bluestein
-    p->bluestein = true;
-    int m = 1;
-    while (m < 2 * n - 1) m <<= 1;
-    p->m = m;
-    p->chirp.resize(n);
-    const long long two_n = 2LL * n;
-    for (long long k = 0; k < n; ++k) {
-        long long e = (k * k) % two_n;  // exact angle reduction: k^2 mod 2n
-        double ang = sign * kPi * (double)e / (double)n;
-        p->chirp[k] = cplx(std::cos(ang), std::sin(ang));
+    if (r > 1) {
+        int m = 1;
+        while (m < 2 * r - 1) m <<= 1;
+        p->m = m;
+        p->chirp.resize(r);
+        const long long two_r = 2LL * r;
+        for (long long k = 0; k < r; ++k) {
+            long long e = (k * k) % two_r;  // exact angle reduction: k^2 mod 2r
+            double ang = sign * kPi * (double)e / (double)r;
+            p->chirp[k] = cplx(std::cos(ang), std::sin(ang));
+        }
+        p->fwd_m = make_plan(m, -1);
+        p->bwd_m = make_plan(m, +1);
+        std::vector<cplx> b(m, cplx(0, 0));
+        b[0] = std::conj(p->chirp[0]);
+        for (int d = 1; d < r; ++d) {
+            b[d] = std::conj(p->chirp[d]);
+            b[m - d] = std::conj(p->chirp[d]);
+        }
+        p->bhat.resize(m);
+        std::vector<cplx> scratch(4 * m + 64);
+        exec_1d(p->fwd_m, b.data(), 1, p->bhat.data(), scratch.data());
     }
-    p->fwd_m = make_plan(m, -1);
-    p->bwd_m = make_plan(m, +1);
-    std::vector<cplx> b(m, cplx(0, 0));
-    b[0] = std::conj(p->chirp[0]);
-    for (int d = 1; d < n; ++d) {
-        b[d] = std::conj(p->chirp[d]);
-        b[m - d] = std::conj(p->chirp[d]);
-    }
-    p->bhat.resize(m);
-    std::vector<cplx> scratch(4 * m + 16);
-    exec_1d(p->fwd_m, b.data(), p->bhat.data(), scratch.data());
     return p;
 }
 
-// Recursive decimation-in-time: out[0..n) = DFT_n of in[0], in[stride], ...
-// tw_step maps this sub-transform's twiddle exponent to the root table of size N.
-void ct_rec(const Plan1D* p, const cplx* in, cplx* out, int n, long stride, int level,
-            long tw_step)
+// Length-`large` DFT of in[0], in[stride], ... by Bluestein.
+void bluestein(const Plan1D* p, const cplx* in, long stride, cplx* out, cplx* scratch)
+{
+    const int r = p->large, m = p->m;
+    cplx* a = scratch;
+    cplx* ahat = scratch + m;
+    cplx* rest = scratch + 2 * m;
+    for (int j = 0; j < r; ++j) a[j] = in[j * stride] * p->chirp[j];
+    for (int j = r; j < m; ++j) a[j] = cplx(0, 0);
+    exec_1d(p->fwd_m, a, 1, ahat, rest);
+    for (int j = 0; j < m; ++j) ahat[j] *= p->bhat[j];
+    exec_1d(p->bwd_m, ahat, 1, a, rest);
+    const double inv_m = 1.0 / (double)m;
+    for (int k = 0; k < r; ++k) out[k] = p->chirp[k] * (a[k] * inv_m);
+}
+
+// out[0..n) = DFT_n of in[0], in[stride], ...; w_n^e = tw[e * tw_step].
+void ct_rec(const Plan1D* p, const cplx* in, long stride, cplx* out, int n, int level,
+            long tw_step, cplx* scratch)
 {
     if (n == 1) {
         out[0] = in[0];
         return;
     }
+    if (level == (int)p->factors.size()) {  // n == p->large
+        bluestein(p, in, stride, out, scratch);
+        return;
+    }
     const int r = p->factors[level];
     const int m = n / r;
     for (int q = 0; q < r; ++q)
-        ct_rec(p, in + q * stride, out + q * m, m, stride * r, level + 1, tw_step * r);
-    const int N = p->n;
-    cplx t[7];
-    cplx y[7];
-    for (int k = 0; k < m; ++k) {
-        // twiddle the r partial transforms
-        for (int q = 0; q < r; ++q) {
-            long e = ((long)q * k * tw_step) % N;
-            t[q] = out[q * m + k] * p->tw[e];
+        ct_rec(p, in + q * stride, stride * r, out + q * m, m, level + 1, tw_step * r, scratch);
+    const cplx* tw = p->tw.data();
+    const long N = p->n;
+    if (r == 2) {
+        for (int k = 0; k < m; ++k) {
+            const cplx a = out[k];
+            const cplx b = out[m + k] * tw[k * tw_step];
+            out[k] = a + b;
+            out[m + k] = a - b;
         }
-        // radix-r DFT over q
+        return;
+    }
+    if (r == 4) {
+        // w_4 = exp(sign*i*pi/2) = sign*i
+        const double sg = (double)p->sign;
+        for (int k = 0; k < m; ++k) {
+            const cplx t0 = out[k];
+            const cplx t1 = out[m + k] * tw[k * tw_step];
+            const cplx t2 = out[2 * m + k] * tw[2 * k * tw_step];
+            const cplx t3 = out[3 * m + k] * tw[3 * k * tw_step];
+            const cplx s02 = t0 + t2, d02 = t0 - t2, s13 = t1 + t3, d13 = t1 - t3;
+            const cplx jd13(-sg * d13.imag(), sg * d13.real());  // (sign*i) * d13
+            out[k] = s02 + s13;
+            out[m + k] = d02 + jd13;
+            out[2 * m + k] = s02 - s13;
+            out[3 * m + k] = d02 - jd13;
+        }
+        return;
+    }
+    cplx t[7], y[7];
+    const long step_r = N / r;  // w_r = tw[step_r]
+    for (int k = 0; k < m; ++k) {
+        for (int q = 0; q < r; ++q) t[q] = out[q * m + k] * tw[(long)q * k * tw_step];
         for (int s = 0; s < r; ++s) {
-            cplx acc(0, 0);
-            for (int q = 0; q < r; ++q) {
-                long e = ((long)q * s * m * tw_step) % N;  // w_r^(q*s)
-                acc += t[q] * p->tw[e];
-            }
+            cplx acc = t[0];
+            for (int q = 1; q < r; ++q) acc += t[q] * tw[((q * s) % r) * step_r];
             y[s] = acc;
         }
         for (int s = 0; s < r; ++s) out[k + s * m] = y[s];
     }
 }
 
-void exec_1d(const Plan1D* p, const cplx* in, cplx* out, cplx* scratch)
+void exec_1d(const Plan1D* p, const cplx* in, long stride, cplx* out, cplx* scratch)
 {
-    const int n = p->n;
-    if (!p->bluestein) {
-        if (n == 1) { out[0] = in[0]; return; }
-        ct_rec(p, in, out, n, 1, 0, 1);
-        return;
-    }
-    const int m = p->m;
-    cplx* a = scratch;         // m
-    cplx* ahat = scratch + m;  // m
-    cplx* rest = scratch + 2 * m;
-    for (int j = 0; j < n; ++j) a[j] = in[j] * p->chirp[j];
-    for (int j = n; j < m; ++j) a[j] = cplx(0, 0);
-    exec_1d(p->fwd_m, a, ahat, rest);
-    for (int j = 0; j < m; ++j) ahat[j] *= p->bhat[j];
-    exec_1d(p->bwd_m, ahat, a, rest);
-    const double inv_m = 1.0 / (double)m;
-    for (int k = 0; k < n; ++k) out[k] = p->chirp[k] * a[k] * inv_m;
+    ct_rec(p, in, stride, out, p->n, 0, 1, scratch);
 }
 
 }  // namespace
@@ -199,27 +206,45 @@ void fftw_execute(const fftw_plan pc)
     if (p->out != p->in) std::memcpy(p->out, p->in, sizeof(cplx) * total);
     cplx* data = p->out;
     const long strides[3] = {n1 * n2, n2, 1};
-    int nthreads = g_nthreads > 0 ? g_nthreads : omp_get_max_threads();
+    const int nthreads = g_nthreads > 0 ? g_nthreads : omp_get_max_threads();
+    // Axis 2 lines are contiguous. For axes 1 and 0, lines that are neighbours along
+    // the contiguous axis are transformed together in tiles of B, so every gathered
+    // cache line serves B transforms.
+    const int B = 8;
     for (int a = 2; a >= 0; --a) {
         const long len = p->n[a];
         if (len <= 1) continue;
         const long stride = strides[a];
         const Plan1D* pl = p->axis[a];
-        const long lines = total / len;
-        const long scratch_len = 4L * (pl->bluestein ? pl->m : len) + 16;
+        const long scratch_len = 4L * (pl->m > 0 ? pl->m : 1) + 64;
+        // tiles: (outer, inner start); inner runs along the contiguous axis
+        const long inner = a == 2 ? 1 : (a == 1 ? n2 : n1 * n2);
+        const long outer = a == 2 ? n0 * n1 : (a == 1 ? n0 : 1);
+        const long tiles_in = a == 2 ? 1 : (inner + B - 1) / B;
+        const long ntiles = outer * tiles_in;
         #pragma omp parallel num_threads(nthreads)
         {
-            std::vector<cplx> line(len), res(len), scratch(scratch_len);
+            std::vector<cplx> tile(len * B), res(len), scratch(scratch_len);
             #pragma omp for schedule(static)
-            for (long l = 0; l < lines; ++l) {
-                // line l: the index with axis a removed, in row-major order
-                long base;
-                if (a == 2) base = l * len;
-                else if (a == 1) base = (l / n2) * (n1 * n2) + (l % n2);
-                else base = l;
-                for (long t = 0; t < len; ++t) line[t] = data[base + t * stride];
-                exec_1d(pl, line.data(), res.data(), scratch.data());
-                for (long t = 0; t < len; ++t) data[base + t * stride] = res[t];
+            for (long tI = 0; tI < ntiles; ++tI) {
+                const long o = tI / tiles_in;
+                if (a == 2) {
+                    cplx* line = data + o * len;
+                    exec_1d(pl, line, 1, res.data(), scratch.data());
+                    std::memcpy(line, res.data(), sizeof(cplx) * len);
+                    continue;
+                }
+                const long i0 = (tI % tiles_in) * B;
+                const int nb = (int)std::min<long>(B, inner - i0);
+                const long base = (a == 1 ? o * n1 * n2 : 0) + i0;
+                for (long t = 0; t < len; ++t)
+                    for (int b = 0; b < nb; ++b) tile[t * B + b] = data[base + t * stride + b];
+                for (int b = 0; b < nb; ++b) {
+                    exec_1d(pl, tile.data() + b, B, res.data(), scratch.data());
+                    for (long t = 0; t < len; ++t) tile[t * B + b] = res[t];
+                }
+                for (long t = 0; t < len; ++t)
+                    for (int b = 0; b < nb; ++b) data[base + t * stride + b] = tile[t * B + b];
             }
         }
     }

@@ -1,0 +1,50 @@
+import importlib
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle")
+for p in (ROOT, ORACLE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    # the CPU checker is test infrastructure; build it if a fresh checkout lacks it
+    if not os.path.exists(os.path.join(ORACLE, "liboracle.so")):
+        subprocess.call(["make", "-s", "-C", ORACLE, "liboracle.so"])
+    if (not os.path.exists(os.path.join(ORACLE, "_ref", "libim3d_ref.so"))
+            and os.path.isdir("/root/reference/header")):
+        subprocess.call(["make", "-s", "-C", ORACLE, "ref"])
+
+
+@pytest.fixture(scope="session")
+def pkg():
+    return importlib.import_module("3dimagetoolkit_b200")
+
+
+@pytest.fixture(scope="session")
+def O():
+    import oracle_py
+
+    return oracle_py
+
+
+@pytest.fixture(scope="session")
+def ctx(pkg):
+    c = pkg.Context(0)
+    yield c
+    c.close()
+
+
+def rel(a, b):
+    import numpy as np
+
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))

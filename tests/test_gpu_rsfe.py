@@ -1,0 +1,101 @@
+"""GPU: segm::rsfe_splitbregman<T>::apply through the C ABI against the CPU checker.
+
+FP64 runs follow the reference's operations and are compared at 1e-9 relative L2
+(the only differences are the convolution's rounding, direct vs FFT, and atan);
+FP32 runs are compared with the FP64 checker at the acceptance bars of the
+workload: u, f1, f2 relative L2 <= 1e-5, sign(phi - alpha) agreement >= 99.9%,
+Dice >= 0.999."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, ls_steps=1, tol=0.0)
+
+
+def _case(pkg, shape=(32, 30, 28), seed=1, r=8.0):
+    u0 = pkg.synth.ellipsoids(shape, seed, n=2, semi_axes=(4, 8))
+    return u0, pkg.synth.sphere_phi0(shape, r)
+
+
+def _both(ctx, pkg, O, u0, phi0, dtype=np.float64, **kw):
+    kw = {**BASE, **kw}
+    got = ctx.rsfe_apply(u0.astype(dtype), None if phi0 is None else phi0.astype(dtype),
+                         pkg.default_params(**kw), want_u=True, want_f=True)
+    want = O.rsfe_apply(u0, phi0, O.default_params(**kw))
+    return got, want
+
+
+@pytest.mark.parametrize("mode", [
+    dict(bc=2), dict(bc=1), dict(), dict(bc=2, sweep=1), dict(bc=1, sweep=1),
+    dict(bc=2, ls_steps=3), dict(bc=2, ls_steps=2, ls_tol=1e-3),
+    dict(bc=2, gs_rel_res_tol=1e-6), dict(bc=1, gs_rel_res_tol=1e-6, omega=1.3),
+    dict(bc=2, init_variables=1), dict(bc=2, lamda1=1.0, lamda2=2.0),
+    dict(bc=2, edge_detector_sigma=1.0), dict(bc=2, gaussian_pixel_approach=1),
+])
+def test_apply_fp64_matches_checker(ctx, pkg, O, mode):
+    u0, phi0 = _case(pkg)
+    got, want = _both(ctx, pkg, O, u0, phi0, maxiter=6, **mode)
+    for key in ("phi", "u", "f1", "f2"):
+        assert rel(got[key], want[key]) < 1e-9, key
+    for key in ("iterations", "total_sweeps", "last_sweeps"):
+        assert got["stats"][key] == want["stats"][key], key
+
+
+def test_apply_cube_init_and_spacing(ctx, pkg, O):
+    u0, _ = _case(pkg, (20, 24, 18))
+    kw = {**BASE, "maxiter": 4, "bc": 2}
+    h = (0.9, 1.0, 1.2)
+    got = ctx.rsfe_apply(u0, None, pkg.default_params(**kw), h=h, want_u=True)
+    want = O.rsfe_apply(u0, None, O.default_params(**kw), h=h)
+    assert rel(got["phi"], want["phi"]) < 1e-9
+    assert rel(got["u"], want["u"]) < 1e-9
+
+
+def test_apply_tolerance_stops_like_checker(ctx, pkg, O):
+    u0, phi0 = _case(pkg, (24, 24, 24))
+    got, want = _both(ctx, pkg, O, u0, phi0, maxiter=200, tol=2e-3, bc=2)
+    assert got["stats"]["iterations"] == want["stats"]["iterations"] < 200
+    assert rel(got["phi"], want["phi"]) < 1e-9
+
+
+def test_config1_fp64_64cube(ctx, pkg, O):
+    """64^3 float64, 2 ellipsoids, sigma 3, 20 outer iterations, 1 sweep each."""
+    u0, phi0 = pkg.synth.config_volume("c1", seed=0)
+    got, want = _both(ctx, pkg, O, u0, -(-phi0), maxiter=20, bc=2)
+    for key in ("phi", "u", "f1", "f2"):
+        assert rel(got[key], want[key]) < 1e-9, key
+
+
+@pytest.mark.parametrize("sweep", [0, 1])
+def test_config1_fp32_acceptance(ctx, pkg, O, sweep):
+    u0, phi0 = pkg.synth.config_volume("c1", seed=0)
+    got, want = _both(ctx, pkg, O, u0, phi0, dtype=np.float32, maxiter=20, bc=2, sweep=sweep)
+    for key in ("u", "f1", "f2"):
+        assert rel(got[key], want[key]) <= 1e-5, key
+    alpha = 0.5
+    agree = np.mean((got["phi"] > alpha) == (want["phi"] > alpha))
+    assert agree >= 0.999
+    assert pkg.synth.dice(got["phi"], want["phi"], alpha) >= 0.999
+
+
+def test_solve_mode_fp32_acceptance(ctx, pkg, O):
+    u0, phi0 = _case(pkg, (48, 44, 40), seed=5, r=12.0)
+    got, want = _both(ctx, pkg, O, u0, phi0, dtype=np.float32, maxiter=15, bc=2,
+                      gs_rel_res_tol=1e-6)
+    assert rel(got["u"], want["u"]) <= 1e-5
+    assert pkg.synth.dice(got["phi"], want["phi"]) >= 0.999
+
+
+def test_invalid_parameters_rejected(ctx, pkg):
+    u0, phi0 = _case(pkg, (8, 8, 8))
+    for bad in (dict(sigma=0.0), dict(lamda=-1.0), dict(dt=0.0), dict(epsilon=0.0),
+                dict(ls_steps=0), dict(bc=7), dict(a0=1.0, b0=0.0)):
+        with pytest.raises(pkg.Im3dError) as e:
+            ctx.rsfe_apply(u0, phi0, pkg.default_params(**bad))
+        assert e.value.status == 1, bad
+    with pytest.raises(pkg.Im3dError) as e:
+        ctx.rsfe_apply(np.zeros((8, 8, 1)), None)
+    assert e.value.status == 2
