@@ -187,6 +187,20 @@ class Context:
             raise Im3dError(st, self.last_error())
         return st
 
+    def set_profiling(self, on: bool = True):
+        self._check(lib().im3d_ctx_set_profiling(self._h, C.c_int(int(on))))
+
+    def profile(self, reset: bool = True) -> dict:
+        """{stage: (total_ms, launches)} accumulated since the last reset."""
+        names = C.create_string_buffer(8192)
+        ms = (C.c_double * 64)()
+        cnt = (C.c_int64 * 64)()
+        n = lib().im3d_ctx_profile(self._h, names, 8192, ms, cnt, 64, int(reset))
+        if n < 0:
+            raise Im3dError(-n, self.last_error())
+        keys = names.value.decode().split("\n")[:n]
+        return {k: (ms[i], int(cnt[i])) for i, k in enumerate(keys)}
+
     def set_stream(self, stream_handle: int | None):
         self._check(lib().im3d_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 

@@ -33,6 +33,20 @@ struct im3d_ctx {
     Ctrl* ctrl_d = nullptr;
     Ctrl* ctrl_h = nullptr;  // pinned
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // per-stage device timing (im3d_ctx_set_profiling): events recorded on the
+    // launching stream around each launch, resolved at the next synchronisation
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    struct Acc {
+        double ms = 0;
+        long long count = 0;
+    };
+    std::vector<std::pair<std::string, Acc>> prof_acc;
 };
 
 namespace {
@@ -67,6 +81,62 @@ int check_launch(im3d_ctx* ctx, const char* what)
         return IM3D_ERR_CUDA;
     }
     return IM3D_OK;
+}
+
+cudaEvent_t prof_event(im3d_ctx* ctx)
+{
+    if (!ctx->ev_pool.empty()) {
+        cudaEvent_t e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Start of a profiled launch: returns the pending slot (-1 when profiling is off).
+int prof_begin(im3d_ctx* ctx, const char* name)
+{
+    if (!ctx->prof) return -1;
+    im3d_ctx::Pending pd{name, prof_event(ctx), prof_event(ctx)};
+    cudaEventRecord(pd.a, ctx->stream);
+    ctx->pending.push_back(pd);
+    return (int)ctx->pending.size() - 1;
+}
+
+void prof_end(im3d_ctx* ctx, int slot)
+{
+    if (slot >= 0) cudaEventRecord(ctx->pending[slot].b, ctx->stream);
+}
+
+// After a stream synchronisation: fold the pending event pairs into the totals.
+void prof_resolve(im3d_ctx* ctx)
+{
+    for (auto& pd : ctx->pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, pd.a, pd.b) != cudaSuccess) {
+            cudaGetLastError();
+            ms = 0;
+        }
+        bool found = false;
+        for (auto& kv : ctx->prof_acc)
+            if (kv.first == pd.name) {
+                kv.second.ms += ms;
+                kv.second.count++;
+                found = true;
+                break;
+            }
+        if (!found) {
+            im3d_ctx::Acc a;
+            a.ms = ms;
+            a.count = 1;
+            ctx->prof_acc.push_back({pd.name, a});
+        }
+        ctx->ev_pool.push_back(pd.a);
+        ctx->ev_pool.push_back(pd.b);
+    }
+    ctx->pending.clear();
 }
 
 // Device buffer of at least `bytes` under `name`, reused across calls.
@@ -154,6 +224,7 @@ int out_finish(im3d_ctx* ctx, T* user, const T* dev, size_t count)
 int sync(im3d_ctx* ctx)
 {
     IM3D_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!ctx->pending.empty()) prof_resolve(ctx);
     return IM3D_OK;
 }
 
@@ -263,7 +334,8 @@ int set_smem(im3d_ctx* ctx, K kernel, size_t bytes)
 }
 
 template <typename T, int N, class Ld, class St>
-int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
+int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
+           const char* name = "conv_k")
 {
     const int S = nh / 2;
     size_t smem = (size_t)RK * (TK + 2 * S) * sizeof(Vec<T, N>) + nh * sizeof(T) + 16;
@@ -271,12 +343,15 @@ int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
     IM3D_TRY(set_smem(ctx, kern, smem));
     long long rows = (long long)d.nx * d.ny;
     dim3 grid((unsigned)((rows + RK - 1) / RK), (d.nz + TK - 1) / TK);
+    const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TK, RK), smem, ctx->stream>>>(ld, st, d, w, nh);
-    return check_launch(ctx, "conv_k");
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
 }
 
 template <typename T, int N, int AXIS, class Ld, class St>
-int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
+int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
+           const char* name = AXIS == 0 ? "conv_s_i" : "conv_s_j")
 {
     constexpr int TA = TileA<T>::v;
     const int S = nh / 2;
@@ -286,8 +361,10 @@ int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh)
     const int len = AXIS == 0 ? d.nx : d.ny;
     const int other = AXIS == 0 ? d.ny : d.nx;
     dim3 grid((d.nz + TW - 1) / TW, (len + TA - 1) / TA, other);
+    const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w, nh);
-    return check_launch(ctx, AXIS == 0 ? "conv_s(i)" : "conv_s(j)");
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
 }
 
 // Scalar Gaussian filter: in -> out through the three passes (tmp1, tmp2 scratch).
@@ -343,6 +420,7 @@ int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c
     const int hix = d.nx - lo, hiy = d.ny - lo, hiz = d.nz - lo;
     if (hix <= lo || hiy <= lo || hiz <= lo) return IM3D_OK;
     const dim3 blk(32, 4);
+    const int pf = prof_begin(ctx, "lex_sweep");
     for (int s = 3 * lo; s <= (hix - 1) + (hiy - 1) + (hiz - 1); ++s) {
         const int i0 = std::max(lo, s - (hiy - 1) - (hiz - 1));
         const int i1 = std::min(hix - 1, s - 2 * lo);
@@ -354,6 +432,7 @@ int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c
         lex_plane_kernel<T><<<grid, blk, 0, ctx->stream>>>(r, b, d, c, s, lo, i0, j0);
         IM3D_TRY(check_launch(ctx, "lex_plane"));
     }
+    prof_end(ctx, pf);
     return IM3D_OK;
 }
 
@@ -362,8 +441,10 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
              double omega)
 {
     for (int color = 0; color < 2; ++color) {
+        const int pf = prof_begin(ctx, "rb_half");
         rb_half_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(U, B, d, c, color,
                                                                           use_self, (T)omega);
+        prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "rb_half"));
     }
     return IM3D_OK;
@@ -399,8 +480,10 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
         ++s;
         if (s % check_every == 0 || s == max_sweeps) {
             IM3D_TRY(zero_ctrl(ctx));
+            const int pf = prof_begin(ctx, "rb_residual");
             rb_residual_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
                 U, B, d, c, ctx->ctrl_d->sum, beff2 < 0 ? 1 : 0);
+            prof_end(ctx, pf);
             IM3D_TRY(check_launch(ctx, "rb_residual"));
             IM3D_TRY(read_ctrl(ctx));
             if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
@@ -562,8 +645,9 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     for (t = 1; tollerance > p->tol && t <= p->maxiter; ++t) {
         // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
         IM3D_TRY((pass_k<T, 4>(ctx, LdHeaviside<T>{phi, u0, d, center, inv_eps}, StVec<T, 4>{W1, d},
-                               d, tp.w[2], tp.nh[2])));
-        IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1])));
+                               d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
+        IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1],
+                                  "conv_s_j4")));
         {
             constexpr int TA = TileA<T>::v;
             const int S = tp.nh[0] / 2;
@@ -572,11 +656,14 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             auto kern = conv_i_fit_kernel<T, TW, TY, TA>;
             IM3D_TRY(set_smem(ctx, kern, smem));
             dim3 grid((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny);
+            const int pf = prof_begin(ctx, "conv_i_fit");
             kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(W2, P1, f1_d, f2_d, d, tp.w[0],
                                                            tp.nh[0], (T)p->lamda1, (T)p->lamda2);
+            prof_end(ctx, pf);
             IM3D_TRY(check_launch(ctx, "conv_i_fit"));
         }
-        IM3D_TRY((pass_s<T, 2, 1>(ctx, LdVec<T, 2>{P1, d}, StVec<T, 2>{P2, d}, d, tp.w[1], tp.nh[1])));
+        IM3D_TRY((pass_s<T, 2, 1>(ctx, LdVec<T, 2>{P1, d}, StVec<T, 2>{P2, d}, d, tp.w[1], tp.nh[1],
+                                  "conv_s_j2")));
         {
             StRhs<T> st;
             st.u0 = u0; st.kones = kones; st.divdb = divdb; st.phi = phi;
@@ -590,7 +677,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             st.bc = (T)chosen_bc;
             st.mode = lex ? 0 : (solve ? 2 : 1);
             st.dirichlet = neu ? 0 : 1;
-            IM3D_TRY((pass_k<T, 2>(ctx, LdVec<T, 2>{P2, d}, st, d, tp.w[2], tp.nh[2])));
+            IM3D_TRY((pass_k<T, 2>(ctx, LdVec<T, 2>{P2, d}, st, d, tp.w[2], tp.nh[2], "conv_k_rhs")));
         }
 
         // the Poisson step (rsfe_splitbregman_imp.hxx:1768-1785)
@@ -643,19 +730,23 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         IM3D_TRY(zero_ctrl(ctx));
         T* phi_new = lex ? other : phi;  // lex: `other` holds phiold and receives the clamp
         const int bregman = init_variables ? 0 : 1;
+        const int pf = prof_begin(ctx, "post_solve");
         if (lex)
             post_solve_kernel<T, false><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
                 uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
         else
             post_solve_kernel<T, true><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
                 uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
+        prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "post_solve"));
         if (init_variables) {
             IM3D_CUDA(ctx, cudaMemsetAsync(divdb, 0, n * sizeof(T), ctx->stream));
             IM3D_CUDA(ctx, cudaMemsetAsync(b3, 0, 3 * n * sizeof(T), ctx->stream));
             init_variables = 0;
         } else {
+            const int pf2 = prof_begin(ctx, "div");
             div_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(dmb, divdb, d, hx, hy, hz);
+            prof_end(ctx, pf2);
             IM3D_TRY(check_launch(ctx, "div"));
         }
         IM3D_TRY(read_ctrl(ctx));
@@ -906,6 +997,41 @@ int im3d_ctx_set_stream(im3d_ctx* ctx, void* stream)
 }
 
 int64_t im3d_ctx_launch_count(const im3d_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int im3d_ctx_set_profiling(im3d_ctx* ctx, int on)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    ctx->prof = on != 0;
+    return IM3D_OK;
+}
+
+int im3d_ctx_profile(im3d_ctx* ctx, char* names, int names_cap, double* ms, int64_t* counts,
+                     int max_entries, int reset)
+{
+    if (!ctx) return -IM3D_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return -IM3D_ERR_CUDA;
+    }
+    prof_resolve(ctx);
+    int n = 0;
+    std::string all;
+    for (auto& kv : ctx->prof_acc) {
+        if (n >= max_entries) break;
+        if (ms) ms[n] = kv.second.ms;
+        if (counts) counts[n] = kv.second.count;
+        all += kv.first;
+        all += '\n';
+        ++n;
+    }
+    if (names && names_cap > 0) {
+        std::strncpy(names, all.c_str(), (size_t)names_cap - 1);
+        names[names_cap - 1] = 0;
+    }
+    if (reset) ctx->prof_acc.clear();
+    return n;
+}
 
 void im3d_rsfe_params_default(im3d_rsfe_params* p)
 {

@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the RSFE Split-Bregman segmentation path on B200.
+
+Metric: Gvoxel-iterations/s = voxels x outer iterations / seconds, whole job.
+Workload (one step): one segmentation of a 256^3 FP32 volume (8 ellipsoids,
+semi-axes 10-40, intensities 0.6-0.9, bias ramp 0.7->1.3 along z, noise 0.05,
+seeded synthetic data), sigma 3, lamda1 = lamda2 = 1, epsilon 1e-3, lamda 0.5,
+Dirichlet boundary, 100 outer iterations, each solving the Poisson step with
+red-black Gauss-Seidel to relative residual 1e-6. The working set (~2 GB) is far
+above the 126 MB L2, so no flush is needed between steps.
+
+Arms:
+  default            the sm_100a library through its C ABI (one rank per GPU under
+                     torchrun; each rank segments its own volume: weak scaling)
+  --impl reference   the reference's own C++ code (oracle/_ref, compiled from the
+                     reference headers with headless shims) on the host cores, one
+                     outer iteration of the same 256^3 workload per step, rank 0 only
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import importlib
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RSFE-SB Gvoxel-iters/s @256^3 (FP32, RB Gauss-Seidel to rel. residual 1e-6)"
+UNIT = "Gvoxel-iters/s"
+SHAPE = (256, 256, 256)
+MAXITER = 100
+PARAMS = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, dt=1.0, a0=0.0,
+              b0=1.0, bc=2, maxiter=MAXITER, tol=0.0, gs_rel_res_tol=1e-6, gs_check_every=2,
+              gs_max_sweeps=1000, omega=1.0)
+
+# Algorithmic bytes per voxel of one launch of each loop kernel (FP32): the
+# compulsory reads and writes of the fields it consumes and produces.
+ALGO_BYTES_PER_VOXEL = {
+    "rb_half": 6.0,           # other colour read 2, own b_eff read 2, own colour write 2
+    "rb_residual": 8.0,       # u read 4, b_eff read 4
+    "conv_k_heaviside": 24.0,  # phi, u0 read 8; four stage-1 fields write 16
+    "conv_s_j4": 32.0,        # four fields read 16, write 16
+    "conv_i_fit": 24.0,       # four fields read 16; the pair (l1 f1 - l2 f2, ...) write 8
+    "conv_s_j2": 16.0,        # pair read 8, write 8
+    "conv_k_rhs": 28.0,       # pair 8, u0 4, div(d-b) 4, phi 4 read; packed b_eff 4, u 4 write
+    "post_solve": 52.0,       # u 4, phiold 4, b 12, g 4 read; phi 4, b 12, d-b 12 write
+    "div": 16.0,              # d-b read 12, div write 4
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except Exception as e:  # nvidia-smi missing: report no clocks
+            log("clock sampler unavailable:", e)
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for r in csv.reader(open(self.path)):
+            if len(r) < 9:
+                continue
+            try:
+                rows.append([x.strip() for x in r])
+            except Exception:
+                pass
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# --------------------------------------------------------------------- GPU arm
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+
+    shape = SHAPE if not args.size else (args.size,) * 3
+    n = shape[0] * shape[1] * shape[2]
+    if args.size:
+        u0_np = pkg.synth.ellipsoids(shape, args.seed + rank, n=8, semi_axes=(10, 40),
+                                     fg_range=(0.6, 0.9), bias=(0.7, 1.3), noise=0.05,
+                                     dtype=np.float32)
+        phi0_np = pkg.synth.sphere_phi0(shape, 20.0, dtype=np.float32)
+    else:
+        u0_np, phi0_np = pkg.synth.config_volume("c2", seed=args.seed + rank, dtype=np.float32)
+    u0_np = np.ascontiguousarray(u0_np, dtype=np.float32)
+    phi0_np = np.ascontiguousarray(phi0_np, dtype=np.float32)
+    dev = torch.device("cuda", local)
+    u0_d = torch.from_numpy(u0_np).to(dev)
+    phi0_d = torch.from_numpy(phi0_np).to(dev)
+    phi_d = torch.empty_like(u0_d)
+    u0_h = torch.from_numpy(u0_np).pin_memory()
+    phi0_h = torch.from_numpy(phi0_np).pin_memory()
+    phi_h = torch.empty(shape, dtype=torch.float32).pin_memory()
+
+    ctx = pkg.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    kw = dict(PARAMS)
+    if args.maxiter:
+        kw["maxiter"] = args.maxiter
+    params = pkg.default_params(**kw)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    stats = {}
+    for _ in range(args.warmup):
+        stats = ctx.rsfe_apply(u0_d, phi0_d, params, phi_out=phi_d)["stats"]
+
+    # device-resident inputs: value
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    launches0 = ctx.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    iters = 0
+    sweeps = 0
+    for _ in range(args.steps):
+        stats = ctx.rsfe_apply(u0_d, phi0_d, params, phi_out=phi_d)["stats"]
+        iters += stats["iterations"]
+        sweeps += stats["total_sweeps"]
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    dt_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    total_vox_iters = sum_over_ranks(float(n) * iters)
+    value = total_vox_iters / (dt_ms * 1e-3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers (H2D in, D2H out)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e_iters = 0
+    for _ in range(args.steps):
+        st = ctx.rsfe_apply(u0_h.numpy(), phi0_h.numpy(), params, phi_out=phi_h.numpy())["stats"]
+        e_iters += st["iterations"]
+    e1.record(stream)
+    barrier()
+    e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e_value = sum_over_ranks(float(n) * e_iters) / (e_ms * 1e-3) / 1e9
+
+    # per-stage device time of one step (profiling pass, after the timed region)
+    ctx.set_profiling(True)
+    ctx.profile(reset=True)
+    ctx.rsfe_apply(u0_d, phi0_d, params, phi_out=phi_d)
+    prof = ctx.profile(reset=True)
+    ctx.set_profiling(False)
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        top = max(prof.items(), key=lambda kv: kv[1][0])
+        name, (ms_total, count) = top
+        avg_s = ms_total / count * 1e-3
+        per_vox = ALGO_BYTES_PER_VOXEL.get(name)
+        achieved = per_vox * n / avg_s / 1e9 if per_vox else None
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic_per_voxel.json")
+        if os.path.exists(tpath):
+            tv = json.load(open(tpath)).get(name)
+            if tv:
+                traffic = float(tv["bytes_per_voxel"]) * n
+        step_ms = prof_total = sum(v[0] for v in prof.values())
+        roofline = {
+            "bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "algo_bytes_per_launch": per_vox * n if per_vox else None,
+            "avg_launch_us": avg_s * 1e6, "launches_per_step": count,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)",
+            "share_of_step": ms_total / prof_total if prof_total else None,
+        }
+        # whole-iteration roofline: algorithmic bytes of every stage over the step time
+        algo_step = sum(ALGO_BYTES_PER_VOXEL.get(k, 0.0) * n * c for k, (m, c) in prof.items())
+        per_step_ms = dt_ms / args.steps
+        roofline["step_algo_gb"] = algo_step / 1e9
+        roofline["step_frac"] = (algo_step / (per_step_ms * 1e-3) / 1e9) / peak
+        stages = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in
+                  sorted(prof.items(), key=lambda kv: -kv[1][0])}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid volumes, one per rank)",
+            "config": {"workload": "rsfe-sb 256^3 fp32, 100 outer iterations, RB-GS to rel. "
+                                   "residual 1e-6", "shape": list(shape), "outer_iterations": MAXITER,
+                       "sigma": 3.0, "volumes_per_rank": 1, "parallelism": f"replicas x{ws} (one volume per GPU)",
+                       "l2": "working set ~2 GB > 126 MB L2, no flush needed",
+                       "gs_sweeps_per_step": sweeps / max(args.steps, 1)},
+            "e2e": {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 4,
+                    "d2h_bytes_per_step": n * 4, "ms_per_step": e_ms / args.steps},
+            "roofline": roofline, "stages_ms_per_step": stages, "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        if ws == 1 and not args.no_cpu:
+            result["cpu_baseline"] = cpu_baseline(args)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+# ------------------------------------------------------------------ CPU arms
+def _ref_iteration_seconds(shape, maxiter, seed):
+    """Wall seconds of each outer iteration after the first, reference code, FP64."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    u0, phi0 = pkg.synth.config_volume("c2", seed=seed, dtype=np.float64)
+    kw = dict(PARAMS)
+    kw["maxiter"] = maxiter
+    p = O.default_params(**kw)
+    O.rsfe_apply(u0, phi0, p, use_reference=True)
+    tl = O.ref_last_timeline()
+    steps = np.diff(tl[1:-1])  # end-of-iteration stamps: intervals are whole iterations
+    return [float(x) for x in steps]
+
+
+def cpu_baseline(args):
+    cores = os.cpu_count()
+    t0 = time.time()
+    secs = _ref_iteration_seconds(SHAPE, 2, args.seed)
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    per_it = statistics.median(secs)
+    log(f"cpu baseline: {len(secs)} timed iteration(s), {per_it:.2f} s each, "
+        f"{time.time() - t0:.1f} s total")
+    return {"value": n / per_it / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "reference C++ (oracle/_ref: the reference headers, FFTW replaced by an "
+                      "in-tree FP64 FFT, VTK/GetPot by headless shims), T=double, 256^3, "
+                      "wall time of outer iteration 2 of 2 (setup and iteration 1 excluded), "
+                      f"OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cores = os.cpu_count()
+    maxiter = 1 + args.warmup + args.steps
+    secs = _ref_iteration_seconds(SHAPE, maxiter, args.seed)
+    timed = secs[args.warmup:args.warmup + args.steps] if len(secs) > args.warmup else secs
+    total = sum(timed)
+    n = SHAPE[0] * SHAPE[1] * SHAPE[2]
+    value = n * len(timed) / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": len(timed), "warmup": args.warmup, "ms_per_step": total / len(timed) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded ellipsoid volume)",
+        "config": {"workload": "rsfe-sb 256^3, one outer iteration per step, Poisson step solved "
+                               "to rel. residual 1e-6 (red-black plug-in)", "shape": list(SHAPE)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{len(timed)} outer iterations of the 256^3 workload after "
+                                   f"{args.warmup} warm-up iterations and the set-up"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--size", type=int, default=0,
+                    help="profiling only: cube side of a smaller/larger case (default 256)")
+    ap.add_argument("--maxiter", type=int, default=0,
+                    help="profiling only: outer iterations per step (default 100)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

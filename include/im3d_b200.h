@@ -107,6 +107,14 @@ const char* im3d_ctx_last_error(const im3d_ctx* ctx);
 int im3d_ctx_set_stream(im3d_ctx* ctx, void* cuda_stream);
 /* Count of kernel launches the context issued since creation (instrumentation). */
 int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
+/* Per-stage device timing: with profiling on, each launch of the loop's kernels is
+ * bracketed by CUDA events on the launching stream. im3d_ctx_profile() synchronises,
+ * writes up to max_entries stage names ('\n'-separated into names), total ms and
+ * launch counts, returns the number of stages (negative status on error) and clears
+ * the totals when reset != 0. No counterpart in the reference (it has no timers). */
+int im3d_ctx_set_profiling(im3d_ctx* ctx, int on);
+int im3d_ctx_profile(im3d_ctx* ctx, char* names, int names_cap, double* ms, int64_t* counts,
+                     int max_entries, int reset);
 
 /* Reference constructor defaults (rsfe_splitbregman_imp.hxx:25-41) plus the
  * extension defaults documented in im3d_rsfe_params. */

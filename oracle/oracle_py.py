@@ -223,3 +223,10 @@ def ref_change_range(x, mx, mn):
     r = _f64(x).copy()
     ref_lib().ref_change_range(_p(r), *map(C.c_int, r.shape), C.c_double(mx), C.c_double(mn))
     return r
+
+
+def ref_last_timeline():
+    """[apply start, end of each outer iteration's Poisson step..., apply end] (s)."""
+    buf = np.zeros(100000)
+    n = ref_lib().ref_last_timeline(_p(buf), C.c_int(buf.size))
+    return buf[:n].copy()

@@ -20,6 +20,7 @@
 
 #include "../im3d_oracle.h"
 
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -61,9 +62,18 @@ struct Recorder
     int last_sweeps = 0;
     double last_rel = -1;
     int not_converged = 0;
+    std::vector<double> stamps;  // wall clock (s) at the end of each Poisson step
 };
 
 Recorder g_rec;
+std::vector<double> g_last_stamps;
+double g_apply_start = 0, g_apply_end = 0;
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
 
 // set_bc takes the class's private enum bc_type by value; the enum is deduced from
 // the public member's signature instead of being named.
@@ -131,6 +141,7 @@ void rec_poisson (img& res, img const& b, double const& dt, double const& bc, im
                     res (i, j, k) = r[ ( (size_t) i * ny + j) * nz + k];
     }
     g_rec.u = res;
+    g_rec.stamps.push_back(now_s() );
 }
 
 }  // namespace
@@ -261,8 +272,11 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     algo.set_epsilon (p->epsilon);
     algo.set_b0 (p->b0);
     algo.set_a0 (p->a0);
-    algo.set_ls_steps (p->ls_steps);
-    algo.set_ls_tol (p->ls_tol);
+    // in the residual mode the plug-in is the whole solve of an outer iteration, so the
+    // reference's sweep loop (:1771-1785) must call it exactly once
+    const bool solve_mode = p->gs_rel_res_tol > 0;
+    algo.set_ls_steps (solve_mode ? 1 : p->ls_steps);
+    algo.set_ls_tol (solve_mode ? 0 : p->ls_tol);
     algo.set_edge_detector_sigma (p->edge_detector_sigma);
     algo.set_gaussian_pixel_approach (p->gaussian_pixel_approach != 0);
     algo.set_cc_init_variables (p->init_variables != 0);
@@ -295,8 +309,11 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     }
     algo.set_onestep_poisson (lapl::unsteady_poisson_functor<double> (rec_poisson) );
 
+    g_apply_start = now_s();
     if (init) algo.apply (u0, phi0);
     else algo.apply (u0);
+    g_apply_end = now_s();
+    g_last_stamps = g_rec.stamps;
 
     img phi = algo.getoutput();
     if (phi_out) from_img (phi_out, phi);
@@ -325,6 +342,19 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     }
     g_rec = Recorder();
     return 0;
+}
+
+/* Timing of the last ref_rsfe_apply: out[0] = start of apply, out[1..n] = wall time
+ * at the end of each outer iteration's Poisson step, out[n+1] = end of apply.
+ * Returns n + 2 (the number of values written, at most cap). */
+int ref_last_timeline (double* out, int cap)
+{
+    int n = 0;
+    if (n < cap) out[n++] = g_apply_start;
+    for (double t : g_last_stamps)
+        if (n < cap) out[n++] = t;
+    if (n < cap) out[n++] = g_apply_end;
+    return n;
 }
 
 }  // extern "C"
