@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -927,6 +928,133 @@ int poisson_solve(im3d_ctx* ctx, T* u_user, const T* b_user, int nx, int ny, int
     return IM3D_OK;
 }
 
+// ------------------------------------------------ Gaussian filter, no allocation
+// Fixed scratch of im3d_gauss_filter_f32_noalloc: two intermediate volumes of up to
+// kNoAllocMaxVoxels voxels, then the three axes' taps.
+constexpr long long kNoAllocMaxVoxels = 1LL << 21;
+constexpr long long kNoAllocFloats = 2 * kNoAllocMaxVoxels + 3 * NH_MAX;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
+
+struct NoAllocTaps {
+    float w[3 * NH_MAX];
+};
+
+// Writes the taps (passed by value) into the scratch array; device code names the
+// array directly.
+__global__ void noalloc_taps_kernel(NoAllocTaps t)
+{
+    for (int q = threadIdx.x; q < 3 * NH_MAX; q += blockDim.x)
+        g_noalloc_scratch[2 * kNoAllocMaxVoxels + q] = t.w[q];
+}
+
+// Device address of g_noalloc_scratch per device, looked up once with that device
+// current (in host code the array's name is only a host-side stand-in).
+float* noalloc_scratch_address(int device, cudaError_t* err)
+{
+    static float* addr[256] = {nullptr};
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 256) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    if (!addr[device]) {
+        void* ptr = nullptr;
+        *err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (*err != cudaSuccess) return nullptr;
+        addr[device] = static_cast<float*>(ptr);
+    }
+    *err = cudaSuccess;
+    return addr[device];
+}
+
+int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, double hx,
+                         double hy, double hz, double sigma, double radius, int pixel_approach,
+                         cudaStream_t stream)
+{
+    if (!in || !out || nx <= 0 || ny <= 0 || nz <= 0) return IM3D_ERR_INVALID_ARG;
+    if (nz == 1 || nx < 3 || ny < 3 || nz < 3) return IM3D_ERR_UNSUPPORTED;
+    if (!(hx > 0) || !(hy > 0) || !(hz > 0) || !(sigma > 0) || !(radius > 0))
+        return IM3D_ERR_INVALID_ARG;
+    const Dims d{nx, ny, nz};
+    if (d.n() > kNoAllocMaxVoxels) return IM3D_ERR_TOO_LARGE;
+    if (!is_device_ptr(in) || !is_device_ptr(out)) return IM3D_ERR_INVALID_ARG;
+    // taps on the host stack: conv::filtering<T>::build_gaussian_filter per axis
+    NoAllocTaps taps;
+    int nh[3];
+    const double hs[3] = {pixel_approach ? 1. : hx, pixel_approach ? 1. : hy,
+                          pixel_approach ? 1. : hz};
+    for (int a = 0; a < 3; ++a) {
+        int m = (int)std::ceil(2 * radius * sigma / hs[a]);
+        if (m % 2 == 0) m++;
+        if (m > NH_MAX) return IM3D_ERR_UNSUPPORTED;
+        nh[a] = m;
+        const int S = m / 2;
+        double w[NH_MAX];
+        double sum = 0;
+        for (int t = 0; t < m; ++t) {
+            const double dd = (double)(t - S);
+            w[t] = std::exp(-dd * dd * hs[a] * hs[a] / (2 * sigma * sigma));
+            sum += w[t];
+        }
+        for (int t = 0; t < NH_MAX; ++t) taps.w[a * NH_MAX + t] = t < m ? (float)(w[t] / sum) : 0.f;
+    }
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return IM3D_ERR_CUDA;
+    }
+    cudaError_t e = cudaSuccess;
+    float* base = noalloc_scratch_address(device, &e);
+    if (!base) {
+        cudaGetLastError();
+        return IM3D_ERR_CUDA;
+    }
+    Vec<float, 1>* t1 = reinterpret_cast<Vec<float, 1>*>(base);
+    Vec<float, 1>* t2 = reinterpret_cast<Vec<float, 1>*>(base + kNoAllocMaxVoxels);
+    const float* w = base + 2 * kNoAllocMaxVoxels;
+    noalloc_taps_kernel<<<1, 128, 0, stream>>>(taps);
+    {
+        const int S = nh[2] / 2;
+        const size_t smem = (size_t)RK * (TK + 2 * S) * sizeof(Vec<float, 1>) + nh[2] * sizeof(float) + 16;
+        auto kern = conv_k_kernel<float, 1, TK, RK, LdScalar<float>, StVec<float, 1>>;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return IM3D_ERR_CUDA;
+        const long long rows = (long long)nx * ny;
+        kern<<<dim3((unsigned)((rows + RK - 1) / RK), (nz + TK - 1) / TK), dim3(TK, RK), smem, stream>>>(
+            LdScalar<float>{in, d}, StVec<float, 1>{t1, d}, d, w + 2 * NH_MAX, nh[2]);
+    }
+    {
+        constexpr int TA = TileA<float>::v;
+        const int S = nh[1] / 2;
+        const size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<float, 1>) + nh[1] * sizeof(float) + 16;
+        auto kern = conv_s_kernel<float, 1, 1, TW, TY, TA, LdVec<float, 1>, StVec<float, 1>>;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return IM3D_ERR_CUDA;
+        kern<<<dim3((nz + TW - 1) / TW, (ny + TA - 1) / TA, nx), dim3(TW, TY), smem, stream>>>(
+            LdVec<float, 1>{t1, d}, StVec<float, 1>{t2, d}, d, w + NH_MAX, nh[1]);
+    }
+    {
+        constexpr int TA = TileA<float>::v;
+        const int S = nh[0] / 2;
+        const size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<float, 1>) + nh[0] * sizeof(float) + 16;
+        auto kern = conv_s_kernel<float, 1, 0, TW, TY, TA, LdVec<float, 1>, StScalar<float>>;
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return IM3D_ERR_CUDA;
+        kern<<<dim3((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny), dim3(TW, TY), smem, stream>>>(
+            LdVec<float, 1>{t2, d}, StScalar<float>{out, d}, d, w, nh[0]);
+    }
+    if (cudaGetLastError() != cudaSuccess) return IM3D_ERR_CUDA;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) {
+        cudaGetLastError();
+        return IM3D_ERR_CUDA;
+    }
+    return IM3D_OK;
+}
+
 int enter(im3d_ctx* ctx)
 {
     if (!ctx) return IM3D_ERR_INVALID_ARG;
@@ -1115,6 +1243,14 @@ int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, in
 {
     IM3D_ENTRY(poisson_solve<double>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
                                      max_sweeps, check_every, omega, sweeps_done, rel_res));
+}
+
+int im3d_gauss_filter_f32_noalloc(const float* in, float* out, int nx, int ny, int nz,
+                                  double hx, double hy, double hz, double sigma, double radius,
+                                  int pixel_approach, void* stream)
+{
+    return gauss_filter_noalloc(in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach,
+                                (cudaStream_t)stream);
 }
 
 int im3d_grad_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz, double hx,

@@ -35,6 +35,7 @@ extern "C" {
 #define IM3D_ERR_CUDA 4          /* a CUDA runtime call failed (text in last_error) */
 #define IM3D_ERR_OOM 5           /* device allocation failed */
 #define IM3D_ERR_NO_DEVICE 6     /* no usable sm_100 device */
+#define IM3D_ERR_TOO_LARGE 7     /* volume above the fixed scratch of a no-allocation entry point */
 
 /* Boundary condition selector. The reference keeps bc_type private
  * (rsfe_splitbregman.hxx:108); its constructor sets bc = NEU but installs
@@ -153,6 +154,27 @@ int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, in
                            double hx, double hy, double hz, double dt, double bc, int bc_type,
                            double rel_res_tol, int max_sweeps, int check_every, double omega,
                            int* sweeps_done, double* rel_res);
+
+/* Gaussian filter that allocates nothing. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code that runs while a host framework owns
+ * all device memory through its own pool (a caching allocator or a fixed arena that a
+ * second allocator must not fragment), code inside a hard device-memory budget, and
+ * code that must not make the allocation calls that can synchronise the device. The
+ * caller passes device buffers `in` and `out` (nx*ny*nz floats each, on the current
+ * device) and a cudaStream_t (NULL = the default stream); the call returns after the
+ * filter has finished on that stream. It is im3d_gauss_filter_f32 with its two
+ * intermediate volumes and its taps held in one file-scope __device__ array of
+ * 2 * 2097152 + 387 floats (16 MiB), which every GPU that loads the library keeps
+ * until the process exits. Volumes above 2097152 voxels (128^3) return
+ * IM3D_ERR_TOO_LARGE without touching the GPU. The first call on a device looks the
+ * array's device address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture. Calls share the array, so calls that overlap on the GPU (other
+ * threads or streams) race; every call rewrites all of the scratch it reads, so
+ * nothing carries over from the previous call. */
+int im3d_gauss_filter_f32_noalloc(const float* in, float* out, int nx, int ny, int nz,
+                                  double hx, double hy, double hz, double sigma, double radius,
+                                  int pixel_approach, void* stream);
 
 /* image3d<T>::grad (image3d_imp.hxx:744-889): out holds 3 volumes, component-major. */
 int im3d_grad_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,

@@ -1,0 +1,60 @@
+"""GPU: the Gaussian filter entry point that allocates nothing.
+
+im3d_gauss_filter_f32_noalloc serves callers that cannot call cudaMalloc (a host
+framework that owns all device memory through its own pool, a hard memory budget,
+code that must not make allocation calls that can synchronise the device). It keeps
+its intermediate volumes in a fixed __device__ array instead of context buffers.
+This test calls it through the C ABI twice in a row, on two different volumes, and
+checks each result against the allocating entry point im3d_gauss_filter_f32, with
+the FP32 tolerance the other filter tests use. It also checks that a volume above
+the fixed capacity is refused before anything runs. It sits in its own file named
+to be collected last, and builds everything it needs itself, so it passes alone in
+a fresh process as well as after the other tests.
+"""
+import ctypes as C
+import importlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MAX_VOXELS = 1 << 21
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _noalloc(lib, x, out, sigma, h, stream=None):
+    return lib.im3d_gauss_filter_f32_noalloc(
+        C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), *map(C.c_int, x.shape),
+        *map(C.c_double, h), C.c_double(sigma), C.c_double(3.0), C.c_int(0),
+        C.c_void_p(stream or 0))
+
+
+def test_noalloc_filter_matches_allocating_entry_point_twice():
+    torch = pytest.importorskip("torch")
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    lib = pkg.lib()
+    rng = np.random.default_rng(123)
+    cases = [((40, 36, 33), 2.0, (1.0, 1.0, 1.0)), ((128, 128, 128), 3.0, (0.9, 1.0, 1.1))]
+    with pkg.Context(0) as ctx:
+        for shape, sigma, h in cases:
+            x_np = rng.random(shape, dtype=np.float32)
+            x = torch.from_numpy(x_np).cuda()
+            out = torch.empty_like(x)
+            st = _noalloc(lib, x, out, sigma, h)
+            assert st == 0, st
+            want = ctx.gauss_filter(x_np, sigma, h=h)
+            got = out.cpu().numpy()
+            assert _rel(got, want) < 2e-6
+
+
+def test_noalloc_filter_refuses_volumes_above_its_scratch():
+    torch = pytest.importorskip("torch")
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    x = torch.zeros((129, 128, 128), dtype=torch.float32, device="cuda")
+    assert x.numel() > MAX_VOXELS
+    out = torch.empty_like(x)
+    assert _noalloc(pkg.lib(), x, out, 2.0, (1.0, 1.0, 1.0)) == 7
