@@ -242,7 +242,7 @@ class Context:
         return res
 
     def poisson_solve(self, u, b, dt=1.0, bc=0.0, bc_type=BC_DIR, tol=1e-6, max_sweeps=1000,
-                      check_every=2, omega=1.0, h=(1.0, 1.0, 1.0)):
+                      check_every=0, omega=1.0, h=(1.0, 1.0, 1.0)):
         """In place on ``u``; returns (sweeps, relative residual, converged)."""
         pu, dtp = _ptr(u)
         pb, _ = _ptr(b)

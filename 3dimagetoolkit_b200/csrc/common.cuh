@@ -19,7 +19,9 @@ namespace im3d {
 struct Dims {
     int nx, ny, nz;
     __host__ __device__ long long n() const { return (long long)nx * ny * nz; }
-    __host__ __device__ int hz() const { return (nz + 1) >> 1; }
+    // packed row pitch: (nz+1)/2 points of one colour, padded to a multiple of 4 so that
+    // every packed row starts 16-byte aligned (padding slots hold no point: k >= nz)
+    __host__ __device__ int hz() const { return (((nz + 1) >> 1) + 3) & ~3; }
     __host__ __device__ long long npk() const { return (long long)nx * ny * hz(); }
     __host__ __device__ long long idx(int i, int j, int k) const
     {
@@ -34,6 +36,34 @@ struct Dims {
 template <typename T, int N>
 struct alignas(sizeof(T) * N <= 16 ? sizeof(T) * N : 16) Vec {
     T v[N];
+};
+
+// 16-byte vector of T: 4 floats or 2 doubles
+template <typename T>
+struct V16;
+template <>
+struct V16<float> {
+    static constexpr int W = 4;
+    typedef float4 type;
+    __device__ static float get(const float4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+    __device__ static void set(float4& v, int c, float x)
+    {
+        if (c == 0) v.x = x;
+        else if (c == 1) v.y = x;
+        else if (c == 2) v.z = x;
+        else v.w = x;
+    }
+};
+template <>
+struct V16<double> {
+    static constexpr int W = 2;
+    typedef double2 type;
+    __device__ static double get(const double2& v, int c) { return c == 0 ? v.x : v.y; }
+    __device__ static void set(double2& v, int c, double x)
+    {
+        if (c == 0) v.x = x;
+        else v.y = x;
+    }
 };
 
 template <typename T, int N>
@@ -76,8 +106,22 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+__device__ __forceinline__ long long block_linear_id()
+{
+    return blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+}
+
+__device__ __forceinline__ long long grid_blocks()
+{
+    return (long long)gridDim.x * gridDim.y * gridDim.z;
+}
+
+// Block sums of one or two doubles, written by thread 0 to this block's slot of
+// `part` (part[b] and, for the second value, part[nblocks + b]). No atomics: a
+// one-block finalize kernel adds the slots in a fixed order, so the totals do not
+// depend on block scheduling.
 template <int NWARPS_MAX = 32>
-__device__ __forceinline__ void block_sum_atomic(double v, double* target)
+__device__ __forceinline__ void block_sum_store(double v, double* part)
 {
     __shared__ double red_sm[NWARPS_MAX];
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -88,13 +132,12 @@ __device__ __forceinline__ void block_sum_atomic(double v, double* target)
     if (tid < 32) {
         double w = (tid < ((nthreads + 31) >> 5)) ? red_sm[tid] : 0.0;
         w = warp_sum(w);
-        if (tid == 0 && w != 0.0) atomicAdd(target, w);
+        if (tid == 0) part[block_linear_id()] = w;
     }
 }
 
-// Two sums at once (halves the barrier count of the tolerance reductions).
 template <int NWARPS_MAX = 32>
-__device__ __forceinline__ void block_sum2_atomic(double a, double b, double* ta, double* tb)
+__device__ __forceinline__ void block_sum2_store(double a, double b, double* part)
 {
     __shared__ double red_a[NWARPS_MAX], red_b[NWARPS_MAX];
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -113,9 +156,29 @@ __device__ __forceinline__ void block_sum2_atomic(double a, double b, double* ta
         wa = warp_sum(wa);
         wb = warp_sum(wb);
         if (tid == 0) {
-            if (wa != 0.0) atomicAdd(ta, wa);
-            if (wb != 0.0) atomicAdd(tb, wb);
+            const long long bid = block_linear_id();
+            part[bid] = wa;
+            part[grid_blocks() + bid] = wb;
         }
+    }
+}
+
+// sums[slot + v] = sum over b of part[v * nblocks + b], v < nvals, in a fixed order.
+__global__ void finalize_sums_kernel(const double* __restrict__ part, long long nblocks, int nvals,
+                                     double* sums, int slot)
+{
+    __shared__ double sm[256];
+    for (int v = 0; v < nvals; ++v) {
+        double acc = 0;
+        for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) acc += part[v * nblocks + b];
+        sm[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) sums[slot + v] = sm[0];
+        __syncthreads();
     }
 }
 

@@ -334,10 +334,27 @@ int set_smem(im3d_ctx* ctx, K kernel, size_t bytes)
     return IM3D_OK;
 }
 
+template <typename T, int N, int S, class Ld, class St>
+int pass_k_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const char* name)
+{
+    constexpr int TKT = 32, RKR = 8, TKW = TKT * 4, SP = (S + 3) & ~3;
+    const size_t smem = (size_t)N * RKR * (TKW + 2 * SP) * sizeof(T);
+    auto kern = conv_k_win_kernel<T, N, S, TKT, RKR, Ld, St>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    const long long rows = (long long)d.nx * d.ny;
+    dim3 grid((unsigned)((rows + RKR - 1) / RKR), (d.nz + TKW - 1) / TKW);
+    const int pf = prof_begin(ctx, name);
+    kern<<<grid, dim3(TKT, RKR), smem, ctx->stream>>>(ld, st, d, w);
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
+}
+
 template <typename T, int N, class Ld, class St>
 int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
            const char* name = "conv_k")
 {
+    if (nh == 19) return pass_k_win<T, N, 9>(ctx, ld, st, d, w, name);
+    if (nh == 25) return pass_k_win<T, N, 12>(ctx, ld, st, d, w, name);
     const int S = nh / 2;
     size_t smem = (size_t)RK * (TK + 2 * S) * sizeof(Vec<T, N>) + nh * sizeof(T) + 16;
     auto kern = conv_k_kernel<T, N, TK, RK, Ld, St>;
@@ -350,10 +367,29 @@ int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
     return check_launch(ctx, name);
 }
 
+template <typename T, int N, int AXIS, int S, class Ld, class St>
+int pass_s_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const char* name)
+{
+    constexpr int R = sizeof(T) == 4 ? 8 : 4;
+    constexpr int TA = TY * R;
+    const size_t smem = (size_t)N * (TA + 2 * S) * TW * sizeof(T);
+    auto kern = conv_s_win_kernel<T, N, AXIS, S, TW, TY, R, Ld, St>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    const int len = AXIS == 0 ? d.nx : d.ny;
+    const int other = AXIS == 0 ? d.ny : d.nx;
+    dim3 grid((d.nz + TW - 1) / TW, (len + TA - 1) / TA, other);
+    const int pf = prof_begin(ctx, name);
+    kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w);
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
+}
+
 template <typename T, int N, int AXIS, class Ld, class St>
 int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
            const char* name = AXIS == 0 ? "conv_s_i" : "conv_s_j")
 {
+    if (nh == 19) return pass_s_win<T, N, AXIS, 9>(ctx, ld, st, d, w, name);
+    if (nh == 25) return pass_s_win<T, N, AXIS, 12>(ctx, ld, st, d, w, name);
     constexpr int TA = TileA<T>::v;
     const int S = nh / 2;
     size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<T, N>) + nh * sizeof(T) + 16;
@@ -366,6 +402,42 @@ int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
     kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w, nh);
     prof_end(ctx, pf);
     return check_launch(ctx, name);
+}
+
+template <typename T, int S>
+int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T* f2,
+                   const Dims& d, const T* w, T l1, T l2)
+{
+    constexpr int TA = TileA<T>::v;
+    constexpr int RA = (TA + 2 * S + TY - 1) / TY;
+    constexpr int H2 = TY * RA, H1 = H2 + 2 * S;
+    const size_t smem = (size_t)(4 * H1 + 2 * H2) * TW * sizeof(T);
+    auto kern = conv_i_fit_win_kernel<T, S, TW, TY, TA>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    dim3 grid((d.nz + TW - 1) / TW, (d.nx + TA - 1) / TA, d.ny);
+    const int pf = prof_begin(ctx, "conv_i_fit");
+    kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(in, out, f1, f2, d, w, l1, l2);
+    prof_end(ctx, pf);
+    return check_launch(ctx, "conv_i_fit");
+}
+
+template <typename T>
+int pass_i_fit(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T* f2, const Dims& d,
+               const T* w, int nh, T l1, T l2)
+{
+    if (nh == 19) return pass_i_fit_win<T, 9>(ctx, in, out, f1, f2, d, w, l1, l2);
+    if (nh == 25) return pass_i_fit_win<T, 12>(ctx, in, out, f1, f2, d, w, l1, l2);
+    constexpr int TA = TileA<T>::v;
+    const int S = nh / 2;
+    size_t smem = (size_t)(TA + 4 * S) * TW * sizeof(Vec<T, 4>) +
+                  (size_t)(TA + 2 * S) * TW * sizeof(Vec<T, 2>) + nh * sizeof(T) + 16;
+    auto kern = conv_i_fit_kernel<T, TW, TY, TA>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    dim3 grid((d.nz + TW - 1) / TW, (d.nx + TA - 1) / TA, d.ny);
+    const int pf = prof_begin(ctx, "conv_i_fit");
+    kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(in, out, f1, f2, d, w, nh, l1, l2);
+    prof_end(ctx, pf);
+    return check_launch(ctx, "conv_i_fit");
 }
 
 // Scalar Gaussian filter: in -> out through the three passes (tmp1, tmp2 scratch).
@@ -406,6 +478,10 @@ GsCoef<T> make_coef(double hx, double hy, double hz, double dt, double bc, int n
     for (int q = 0; q < 4; ++q) c.bcnd[q] = (double)c.bcn[q];
     c.bc = tb;
     c.neu = neu;
+    c.ihx2d = 1.0 / (hx * hx);
+    c.ihy2d = 1.0 / (hy * hy);
+    c.ihz2d = 1.0 / (hz * hz);
+    c.diagd = 1.0 / dt + 2.0 * c.ihx2d + 2.0 * c.ihy2d + 2.0 * c.ihz2d;
     return c;
 }
 
@@ -437,18 +513,81 @@ int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c
     return IM3D_OK;
 }
 
+constexpr int kNI = 8;  // planes per thread of the scalar column-marching kernels
+constexpr int kNV = 2;  // planes per thread of the vectorised kernels (measured best on B200)
+const dim3 kBlkVec(32, 4, 1);
+
+dim3 grid_col_pk(const Dims& d, dim3 blk, int zmul = 1)
+{
+    return dim3((d.hz() + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y,
+                ((d.nx + kNI - 1) / kNI) * zmul);
+}
+
+// vector groups of 16 bytes along the packed rows
+template <typename T>
+dim3 grid_vec_pk(const Dims& d, dim3 blk, int zmul = 1)
+{
+    const int groups = d.hz() / V16<T>::W;
+    return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y,
+                ((d.nx + kNV - 1) / kNV) * zmul);
+}
+
+template <typename T>
+dim3 grid_vec(const Dims& d, dim3 blk)
+{
+    const int groups = d.nz / V16<T>::W;
+    return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNV - 1) / kNV);
+}
+
+dim3 grid_col(const Dims& d, dim3 blk)
+{
+    return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNI - 1) / kNI);
+}
+
 template <typename T>
 int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, int use_self,
              double omega)
 {
     for (int color = 0; color < 2; ++color) {
         const int pf = prof_begin(ctx, "rb_half");
-        rb_half_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(U, B, d, c, color,
-                                                                          use_self, (T)omega);
+        rb_half_vec_kernel<T, kNV><<<grid_vec_pk<T>(d, kBlkVec), kBlkVec, 0, ctx->stream>>>(
+            U, B, d, c, color, use_self, (T)omega);
         prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "rb_half"));
     }
     return IM3D_OK;
+}
+
+// Per-block partial sums of a reduction launch (nvals values per block).
+int part_buf(im3d_ctx* ctx, dim3 grid, int nvals, double** out)
+{
+    const long long nb = (long long)grid.x * grid.y * grid.z;
+    return tbuf<double>(ctx, "partials", (size_t)(nb * nvals), out);
+}
+
+// Folds the partials of the last reduction launch into ctrl->sum[slot .. slot+nvals).
+int finalize(im3d_ctx* ctx, const double* part, dim3 grid, int nvals, int slot)
+{
+    const long long nb = (long long)grid.x * grid.y * grid.z;
+    finalize_sums_kernel<<<1, 256, 0, ctx->stream>>>(part, nb, nvals, ctx->ctrl_d->sum, slot);
+    return check_launch(ctx, "finalize_sums");
+}
+
+// Next residual check of the Poisson solve. check_every > 0: a fixed interval.
+// check_every == 0: first checks after 4 and 8 sweeps, then the remaining sweeps are
+// predicted from the contraction between the last two checks,
+//   rate = (r_s / r_prev)^(1/(s - s_prev)),  need = log(tol / r_s) / log(rate),
+// and the next check is ceil(need) sweeps later, clamped to [1, 32].
+int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every)
+{
+    if (check_every > 0) return s + check_every;
+    if (s_prev <= 0 || !(r_prev > r_s) || !(r_s > 0)) return s + 4;
+    const double rate = std::pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    const double need = std::log(tol / r_s) / std::log(rate);
+    int step = 32;
+    if (need == need && need < 32.0) step = (int)std::ceil(need);
+    if (step < 1) step = 1;
+    return s + step;
 }
 
 int zero_ctrl(im3d_ctx* ctx)
@@ -470,30 +609,41 @@ template <typename T>
 int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, double tol,
              int max_sweeps, int check_every, double omega, int* sweeps, double* rel, bool* conv)
 {
-    if (check_every < 1) check_every = 1;
+    if (check_every < 0) check_every = 0;
     if (max_sweeps < 1) max_sweeps = 1;
     double beff2 = -1;
-    int s = 0;
+    int s = 0, s_prev = 0;
+    double r_prev = -1;
+    int next = check_every > 0 ? check_every : 4;
     *conv = false;
     *rel = -1;
     while (s < max_sweeps) {
         IM3D_TRY(rb_sweep(ctx, U, B, d, c, 0, omega));
         ++s;
-        if (s % check_every == 0 || s == max_sweeps) {
-            IM3D_TRY(zero_ctrl(ctx));
+        if (s >= next || s == max_sweeps) {
+            const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2);
+            const int nvals = beff2 < 0 ? 2 : 1;
+            double* part = nullptr;
+            IM3D_TRY(part_buf(ctx, grid, nvals, &part));
             const int pf = prof_begin(ctx, "rb_residual");
-            rb_residual_kernel<T><<<grid_pk(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
-                U, B, d, c, ctx->ctrl_d->sum, beff2 < 0 ? 1 : 0);
+            rb_residual_vec_kernel<T, kNV><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part,
+                                                                            nvals == 2 ? 1 : 0);
             prof_end(ctx, pf);
             IM3D_TRY(check_launch(ctx, "rb_residual"));
+            IM3D_TRY(finalize(ctx, part, grid, nvals, SUM_RES2));
             IM3D_TRY(read_ctrl(ctx));
             if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
             const double rr = ctx->ctrl_h->sum[SUM_RES2];
-            *rel = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
-            if (*rel <= tol) {
+            const double r = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
+            *rel = r;
+            if (r <= tol) {
                 *conv = true;
                 break;
             }
+            next = next_check(s, r, s_prev, r_prev, tol, check_every);
+            if (next > max_sweeps) next = max_sweeps;
+            s_prev = s;
+            r_prev = r;
         }
     }
     *sweeps = s;
@@ -649,20 +799,8 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                                d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
         IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1],
                                   "conv_s_j4")));
-        {
-            constexpr int TA = TileA<T>::v;
-            const int S = tp.nh[0] / 2;
-            size_t smem = (size_t)(TA + 4 * S) * TW * sizeof(Vec<T, 4>) +
-                          (size_t)(TA + 2 * S) * TW * sizeof(Vec<T, 2>) + tp.nh[0] * sizeof(T) + 16;
-            auto kern = conv_i_fit_kernel<T, TW, TY, TA>;
-            IM3D_TRY(set_smem(ctx, kern, smem));
-            dim3 grid((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny);
-            const int pf = prof_begin(ctx, "conv_i_fit");
-            kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(W2, P1, f1_d, f2_d, d, tp.w[0],
-                                                           tp.nh[0], (T)p->lamda1, (T)p->lamda2);
-            prof_end(ctx, pf);
-            IM3D_TRY(check_launch(ctx, "conv_i_fit"));
-        }
+        IM3D_TRY(pass_i_fit<T>(ctx, W2, P1, f1_d, f2_d, d, tp.w[0], tp.nh[0], (T)p->lamda1,
+                               (T)p->lamda2));
         IM3D_TRY((pass_s<T, 2, 1>(ctx, LdVec<T, 2>{P1, d}, StVec<T, 2>{P2, d}, d, tp.w[1], tp.nh[1],
                                   "conv_s_j2")));
         {
@@ -712,10 +850,12 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                 if (lex) IM3D_TRY(lex_sweep<T>(ctx, phi, rhs, d, coef));
                 else IM3D_TRY(rb_sweep<T>(ctx, upk, bpk, d, coef, 1, 1.0));
                 if (p->ls_tol != 0 && s >= p->ls_steps - 1) {
-                    IM3D_TRY(zero_ctrl(ctx));
-                    diff_sums_kernel<T><<<flat_grid(cnt), 256, 0, ctx->stream>>>(work, prev, cnt,
-                                                                               ctx->ctrl_d->sum);
+                    const dim3 grid(flat_grid(cnt));
+                    double* part = nullptr;
+                    IM3D_TRY(part_buf(ctx, grid, 2, &part));
+                    diff_sums_kernel<T><<<grid, 256, 0, ctx->stream>>>(work, prev, cnt, part);
                     IM3D_TRY(check_launch(ctx, "diff_sums"));
+                    IM3D_TRY(finalize(ctx, part, grid, 2, SUM_A));
                     IM3D_TRY(read_ctrl(ctx));
                     ls_err = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_A]) /
                              std::sqrt(hhh * ctx->ctrl_h->sum[SUM_B]);
@@ -728,25 +868,51 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         }
 
         // clamp, tolerance, Bregman update, div(d - b)
-        IM3D_TRY(zero_ctrl(ctx));
         T* phi_new = lex ? other : phi;  // lex: `other` holds phiold and receives the clamp
-        const int bregman = init_variables ? 0 : 1;
-        const int pf = prof_begin(ctx, "post_solve");
-        if (lex)
-            post_solve_kernel<T, false><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
-                uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
-        else
-            post_solve_kernel<T, true><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
-                uu, phi_new, u_d, b3, dmb, g, d, hx, hy, hz, a0, b0, bregman, ctx->ctrl_d->sum);
-        prof_end(ctx, pf);
-        IM3D_TRY(check_launch(ctx, "post_solve"));
+        // vector path: rows 16-byte aligned (nz multiple of the width) and an aligned u_out
+        const bool vec = d.nz % V16<T>::W == 0 && ((uintptr_t)u_d % 16) == 0;
+        {
+            const dim3 grid = vec ? grid_vec<T>(d, kBlkVec) : grid_col(d, kBlkVol);
+            const dim3 blk = vec ? kBlkVec : kBlkVol;
+            double* part = nullptr;
+            IM3D_TRY(part_buf(ctx, grid, 2, &part));
+            const int pf = prof_begin(ctx, "clamp_tol");
+            if (vec && lex)
+                clamp_tol_vec_kernel<T, false, kNV><<<grid, blk, 0, ctx->stream>>>(
+                    uu, phi_new, u_d, d, a0, b0, part);
+            else if (vec)
+                clamp_tol_vec_kernel<T, true, kNV><<<grid, blk, 0, ctx->stream>>>(
+                    uu, phi_new, u_d, d, a0, b0, part);
+            else if (lex)
+                clamp_tol_kernel<T, false, kNI><<<grid, kBlkVol, 0, ctx->stream>>>(
+                    uu, phi_new, u_d, d, a0, b0, part);
+            else
+                clamp_tol_kernel<T, true, kNI><<<grid, kBlkVol, 0, ctx->stream>>>(
+                    uu, phi_new, u_d, d, a0, b0, part);
+            prof_end(ctx, pf);
+            IM3D_TRY(check_launch(ctx, "clamp_tol"));
+            IM3D_TRY(finalize(ctx, part, grid, 2, SUM_DPHI2));
+        }
         if (init_variables) {
             IM3D_CUDA(ctx, cudaMemsetAsync(divdb, 0, n * sizeof(T), ctx->stream));
             IM3D_CUDA(ctx, cudaMemsetAsync(b3, 0, 3 * n * sizeof(T), ctx->stream));
             init_variables = 0;
         } else {
+            const int pf = prof_begin(ctx, "bregman");
+            if (vec)
+                bregman_vec_kernel<T, kNV><<<grid_vec<T>(d, kBlkVec), kBlkVec, 0, ctx->stream>>>(
+                    phi_new, b3, dmb, g, d, hx, hy, hz);
+            else
+                bregman_kernel<T, kNI><<<grid_col(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+                    phi_new, b3, dmb, g, d, hx, hy, hz);
+            prof_end(ctx, pf);
+            IM3D_TRY(check_launch(ctx, "bregman"));
             const int pf2 = prof_begin(ctx, "div");
-            div_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(dmb, divdb, d, hx, hy, hz);
+            if (vec)
+                div_vec_kernel<T, kNV><<<grid_vec<T>(d, kBlkVec), kBlkVec, 0, ctx->stream>>>(
+                    dmb, divdb, d, hx, hy, hz);
+            else
+                div_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(dmb, divdb, d, hx, hy, hz);
             prof_end(ctx, pf2);
             IM3D_TRY(check_launch(ctx, "div"));
         }
@@ -909,9 +1075,9 @@ int poisson_solve(im3d_ctx* ctx, T* u_user, const T* b_user, int nx, int ny, int
     IM3D_TRY(tbuf<T>(ctx, "op_bpk", 2 * d.npk(), &B, true));
     pack_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(r, U, d);
     IM3D_TRY(check_launch(ctx, "pack"));
-    IM3D_TRY(zero_ctrl(ctx));
-    make_beff_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
-        b, U, B, d, (T)(1.0 / dt), (T)bc, neu ? 0 : 1, ctx->ctrl_d->sum);
+    make_beff_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(b, U, B, d,
+                                                                          (T)(1.0 / dt), (T)bc,
+                                                                          neu ? 0 : 1, nullptr);
     IM3D_TRY(check_launch(ctx, "make_beff"));
     int sw = 0;
     double rel = -1;
@@ -1189,7 +1355,7 @@ void im3d_rsfe_params_default(im3d_rsfe_params* p)
     p->gs_rel_res_tol = 0;
     p->omega = 1.0;
     p->gs_max_sweeps = 1000;
-    p->gs_check_every = 2;
+    p->gs_check_every = 0;
 }
 
 #define IM3D_ENTRY(...)                \

@@ -247,6 +247,260 @@ __global__ void __launch_bounds__(TW* TY) conv_s_kernel(Ld ld, St st, Dims d, co
     }
 }
 
+// ---- register-window passes for a compile-time half width S (taps 2S+1) ----
+// Each thread computes R consecutive outputs along the convolution axis from a
+// register window of R + 2S inputs, with the taps in registers and the inputs in
+// shared memory as one plane per field; this reads each staged input (R+2S)/R times
+// instead of 2S+1 times.
+template <typename T, int S, int R>
+__device__ __forceinline__ void window_conv(const T (&x)[R + 2 * S], const T (&w)[S + 1],
+                                            T (&out)[R])
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        T acc = w[S] * x[r + S];
+#pragma unroll
+        for (int t = 0; t < S; ++t) acc = fma(w[t], x[r + t] + x[r + 2 * S - t], acc);
+        out[r] = acc;
+    }
+}
+
+template <typename T, int S>
+__device__ __forceinline__ void load_taps(const T* __restrict__ taps, T (&w)[S + 1])
+{
+#pragma unroll
+    for (int t = 0; t <= S; ++t) w[t] = __ldg(taps + t);
+}
+
+// Along k (contiguous). Block TKT x RKR threads; each thread 4 consecutive k of one
+// row; tile RKR rows x 4*TKT k. The halo is rounded up to SP = 4*ceil(S/4) so that
+// every thread's window starts 16-byte aligned and is read with vector loads.
+template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
+__global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims d,
+                                                            const T* __restrict__ taps)
+{
+    constexpr int R = 4;
+    constexpr int TK = TKT * R;
+    constexpr int SP = (S + 3) & ~3;
+    constexpr int W = TK + 2 * SP;
+    constexpr int XW = R + 2 * SP;  // window read by one thread
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);  // [N][RKR][W]
+    const long long row = (long long)blockIdx.x * RKR + threadIdx.y;
+    const bool live = row < (long long)d.nx * d.ny;
+    const int i = live ? (int)(row / d.ny) : 0;
+    const int j = live ? (int)(row % d.ny) : 0;
+    const int k0 = blockIdx.y * TK;
+    {
+        constexpr int NL = (W + TKT - 1) / TKT;
+        Vec<T, N> v[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.x + u * TKT;
+            const int k = k0 - SP + s;
+            v[u] = (s < W && live && k >= 0 && k < d.nz) ? ld(i, j, k) : vzero<T, N>();
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.x + u * TKT;
+            if (s < W) {
+#pragma unroll
+                for (int q = 0; q < N; ++q) sm[(q * RKR + threadIdx.y) * W + s] = v[u].v[q];
+            }
+        }
+    }
+    T w[S + 1];
+    load_taps<T, S>(taps, w);
+    __syncthreads();
+    const int kk = k0 + threadIdx.x * R;
+    if (!live || kk >= d.nz) return;
+    Vec<T, N> out[R];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        const T* base = sm + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
+        T xa[XW];
+        if (sizeof(T) == 4) {
+#pragma unroll
+            for (int t = 0; t < XW; t += 4) {
+                const float4 v4 = *reinterpret_cast<const float4*>(base + t);
+                xa[t] = v4.x; xa[t + 1] = v4.y; xa[t + 2] = v4.z; xa[t + 3] = v4.w;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < XW; t += 2) {
+                const double2 v2 = *reinterpret_cast<const double2*>(base + t);
+                xa[t] = v2.x; xa[t + 1] = v2.y;
+            }
+        }
+        T x[R + 2 * S];
+#pragma unroll
+        for (int t = 0; t < R + 2 * S; ++t) x[t] = xa[t + SP - S];
+        T o[R];
+        window_conv<T, S, R>(x, w, o);
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[r].v[q] = o[r];
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (kk + r < d.nz) st(i, j, kk + r, out[r]);
+}
+
+// Along j (AXIS 1) or i (AXIS 0). Block TW x TY; each thread R consecutive outputs
+// along the axis in one k column; tile TY*R along the axis x TW along k.
+template <typename T, int N, int AXIS, int S, int TW, int TY, int R, class Ld, class St>
+__global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d,
+                                                          const T* __restrict__ taps)
+{
+    constexpr int TA = TY * R;
+    constexpr int H = TA + 2 * S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sm = reinterpret_cast<T*>(smem_raw);  // [N][H][TW]
+    const int k = blockIdx.x * TW + threadIdx.x;
+    const int a0 = blockIdx.y * TA;
+    const int other = blockIdx.z;
+    const int len = AXIS == 0 ? d.nx : d.ny;
+    const bool kin = k < d.nz;
+    {
+        constexpr int NL = (H + TY - 1) / TY;
+        Vec<T, N> v[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.y + u * TY;
+            const int a = a0 - S + s;
+            v[u] = vzero<T, N>();
+            if (s < H && kin && a >= 0 && a < len) v[u] = AXIS == 0 ? ld(a, other, k) : ld(other, a, k);
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.y + u * TY;
+            if (s < H) {
+#pragma unroll
+                for (int q = 0; q < N; ++q) sm[(q * H + s) * TW + threadIdx.x] = v[u].v[q];
+            }
+        }
+    }
+    T w[S + 1];
+    load_taps<T, S>(taps, w);
+    __syncthreads();
+    if (!kin) return;
+    const int r0 = threadIdx.y * R;
+    Vec<T, N> out[R];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        T x[R + 2 * S];
+#pragma unroll
+        for (int t = 0; t < R + 2 * S; ++t) x[t] = sm[(q * H + r0 + t) * TW + threadIdx.x];
+        T o[R];
+        window_conv<T, S, R>(x, w, o);
+#pragma unroll
+        for (int r = 0; r < R; ++r) out[r].v[q] = o[r];
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int a = a0 + r0 + r;
+        if (a < len) {
+            if (AXIS == 0) st(a, other, k, out[r]);
+            else st(other, a, k, out[r]);
+        }
+    }
+}
+
+// Fused i-axis stage with register windows (see conv_i_fit_kernel for the maths).
+// First pass: RA = ceil((TA+2S)/TY) rows per thread over the four fields; second
+// pass: RB = TA/TY rows per thread over the pair.
+template <typename T, int S, int TW, int TY, int TA>
+__global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>* __restrict__ in,
+                                                              Vec<T, 2>* __restrict__ out,
+                                                              T* f1_out, T* f2_out, Dims d,
+                                                              const T* __restrict__ taps, T l1,
+                                                              T l2)
+{
+    constexpr int RA = (TA + 2 * S + TY - 1) / TY;
+    constexpr int RB = TA / TY;
+    constexpr int H2 = TY * RA;          // rows of the first pass's output (>= TA + 2S)
+    constexpr int H1 = H2 + 2 * S;       // input rows
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sin = reinterpret_cast<T*>(smem_raw);   // [4][H1][TW]
+    T* smid = sin + 4 * H1 * TW;               // [2][H2][TW]
+    const int k = blockIdx.x * TW + threadIdx.x;
+    const int i0 = blockIdx.y * TA;
+    const int j = blockIdx.z;
+    const bool kin = k < d.nz;
+    {
+        constexpr int NL = (H1 + TY - 1) / TY;
+        Vec<T, 4> v[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.y + u * TY;
+            const int i = i0 - 2 * S + s;
+            v[u] = vzero<T, 4>();
+            if (s < H1 && kin && i >= 0 && i < d.nx) v[u] = in[d.idx(i, j, k)];
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int s = threadIdx.y + u * TY;
+            if (s < H1) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sin[(q * H1 + s) * TW + threadIdx.x] = v[u].v[q];
+            }
+        }
+    }
+    T w[S + 1];
+    load_taps<T, S>(taps, w);
+    __syncthreads();
+    {
+        const int r0 = threadIdx.y * RA;
+        T c[4][RA];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            T x[RA + 2 * S];
+#pragma unroll
+            for (int t = 0; t < RA + 2 * S; ++t) x[t] = sin[(q * H1 + r0 + t) * TW + threadIdx.x];
+            window_conv<T, S, RA>(x, w, c[q]);
+        }
+#pragma unroll
+        for (int r = 0; r < RA; ++r) {
+            const int s = r0 + r;           // first-pass row: i = i0 - S + s
+            const int i = i0 - S + s;
+            T pv = T(0), qv = T(0);
+            if (kin && i >= 0 && i < d.nx) {
+                const T f1 = c[0][r] / c[1][r];
+                const T f2 = c[2][r] / c[3][r];
+                pv = f1 * l1 - f2 * l2;
+                qv = (f1 * f1) * l1 - (f2 * f2) * l2;
+                if (f1_out && s >= S && s < S + TA) {
+                    const long long qq = d.idx(i, j, k);
+                    f1_out[qq] = f1;
+                    f2_out[qq] = f2;
+                }
+            }
+            smid[(0 * H2 + s) * TW + threadIdx.x] = pv;
+            smid[(1 * H2 + s) * TW + threadIdx.x] = qv;
+        }
+    }
+    __syncthreads();
+    if (!kin) return;
+    const int r0 = threadIdx.y * RB;
+    T o[2][RB];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        T x[RB + 2 * S];
+#pragma unroll
+        for (int t = 0; t < RB + 2 * S; ++t) x[t] = smid[(q * H2 + r0 + t) * TW + threadIdx.x];
+        window_conv<T, S, RB>(x, w, o[q]);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; ++r) {
+        const int i = i0 + r0 + r;
+        if (i < d.nx) {
+            Vec<T, 2> v;
+            v.v[0] = o[0][r];
+            v.v[1] = o[1][r];
+            out[d.idx(i, j, k)] = v;
+        }
+    }
+}
+
 // Fused i-axis stage: K_i applied to the four stage-1 fields (H u0, H, Hb u0, Hb)
 // completes num, den, numb, denb; then f1 = num/den, f2 = numb/denb, the second
 // pair (l1 f1 - l2 f2, l1 f1^2 - l2 f2^2) is formed and K_i is applied to it.
@@ -400,86 +654,6 @@ __global__ void edge_kernel(const T* __restrict__ f, T* __restrict__ g, Dims d, 
     g[p] = r;
 }
 
-// Clamped level-set value at a point, read from the natural or the packed layout.
-template <typename T, bool PACKED>
-__device__ __forceinline__ T phi_at(const T* u, const Dims& d, int i, int j, int k, T a0, T b0)
-{
-    T v;
-    if (PACKED) v = u[d.pidx(i, j, k) + (((i + j + k) & 1) ? d.npk() : 0)];
-    else v = u[d.idx(i, j, k)];
-    if (v < a0) v = a0;
-    else if (v > b0) v = b0;
-    return v;
-}
-
-template <typename T, bool PACKED>
-__device__ __forceinline__ T grad_phi(const T* u, const Dims& d, int i, int j, int k, int axis,
-                                      double h, T a0, T b0)
-{
-    const int len = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
-    const int pos = axis == 0 ? i : (axis == 1 ? j : k);
-    auto at = [&](int o) {
-        return axis == 0 ? phi_at<T, PACKED>(u, d, i + o, j, k, a0, b0)
-                         : (axis == 1 ? phi_at<T, PACKED>(u, d, i, j + o, k, a0, b0)
-                                      : phi_at<T, PACKED>(u, d, i, j, k + o, a0, b0));
-    };
-    if (pos == 0) return (T(4) * at(1) - T(3) * at(0) - at(2)) / T(2. * h);
-    if (pos == len - 1) return (T(3) * at(0) - T(4) * at(-1) + at(-2)) / T(2. * h);
-    return (at(1) - at(-1)) / T(2. * h);
-}
-
-// After the Poisson step: cut_phi (clamp to [a0, b0]), the tolerance sums
-// sum (phi - phiold)^2 and sum phiold^2, and -- unless bregman == 0 -- the
-// Split-Bregman update per component c (rsfe_splitbregman_imp.hxx:1868-1906):
-//   d = grad(phi)_c; b += d; d = shrink(b, g); b -= d; d -= b
-// The new d (= d_new - b_new) goes to dmb for the divergence kernel.
-// `phi` holds phiold on entry and the clamped phi on exit (each thread reads and
-// writes only its own point there); the neighbours come from u.
-template <typename T, bool PACKED>
-__global__ void post_solve_kernel(const T* __restrict__ u, T* phi, T* __restrict__ u_out,
-                                  T* __restrict__ b3, T* __restrict__ dmb,
-                                  const T* __restrict__ g, Dims d, double hx, double hy,
-                                  double hz, T a0, T b0, int bregman, double* sums)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    double s_d = 0, s_o = 0;
-    if (k < d.nz && j < d.ny) {
-        const long long p = d.idx(i, j, k);
-        T uv;
-        if (PACKED) uv = u[d.pidx(i, j, k) + (((i + j + k) & 1) ? d.npk() : 0)];
-        else uv = u[p];
-        if (u_out) u_out[p] = uv;
-        T v = uv;
-        if (v < a0) v = a0;
-        else if (v > b0) v = b0;
-        const T old = phi[p];
-        phi[p] = v;
-        const double df = (double)v - (double)old;
-        s_d = df * df;
-        s_o = (double)old * (double)old;
-        if (bregman) {
-            const long long n = d.n();
-            const T gg = g[p];
-            const double hs[3] = {hx, hy, hz};
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const T dc = grad_phi<T, PACKED>(u, d, i, j, k, c, hs[c], a0, b0);
-                T bb = b3[c * n + p];
-                bb += dc;
-                const T m = fabs(bb) - gg;
-                const T sgn = T((int)(bb > T(0)) - (int)(bb < T(0)));
-                const T dn = sgn * ((m < T(0)) ? T(0) : m);
-                bb -= dn;
-                b3[c * n + p] = bb;
-                dmb[c * n + p] = dn - bb;
-            }
-        }
-    }
-    block_sum2_atomic(s_d, s_o, sums + SUM_DPHI2, sums + SUM_PHIOLD2);
-}
-
 // ------------------------------------------------------------- Gauss-Seidel
 template <typename T>
 struct GsCoef {
@@ -492,6 +666,8 @@ struct GsCoef {
     double bcnd[4];
     T bc;
     int neu;
+    // FP64 forms for the residual: 1/h^2 and the diagonal 1/dt + 2/hx^2 + 2/hy^2 + 2/hz^2
+    double ihx2d, ihy2d, ihz2d, diagd;
 };
 
 // One Gauss-Seidel point value (sum of neighbour terms + b + self/dt) * htilde;
@@ -586,33 +762,6 @@ __global__ void dir_faces_kernel(T* r, Dims d, T bc)
         r[d.idx(i, j, k)] = bc;
 }
 
-// Red-black half sweep on the colour-packed layout: updates colour `color`, reading
-// the other colour. Thread per packed (m, j, i). Modes:
-//   use_self = 1: reference sweep formula (b + self/dt), b packed rhs;
-//   use_self = 0: fixed u_in, b = b_eff packed; omega != 1 over-relaxes.
-template <typename T>
-__global__ void rb_half_kernel(T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c,
-                               int color, int use_self, T omega)
-{
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (j >= d.ny) return;
-    const int k = 2 * m + ((i + j + color) & 1);
-    if (k >= d.nz) return;
-    const int lo = c.neu ? 0 : 1;
-    if (i < lo || j < lo || k < lo || i >= d.nx - lo || j >= d.ny - lo || k >= d.nz - lo) return;
-    const long long npk = d.npk();
-    T* own = U + (color ? npk : 0);
-    const T* oth = U + (color ? 0 : npk);
-    const long long pq = d.pidx(i, j, k);
-    auto rd = [&](int oi, int oj, int ok) { return oth[d.pidx(i + oi, j + oj, k + ok)]; };
-    const T self = (use_self || omega != T(1)) ? own[pq] : T(0);
-    T v = gs_value<T>(c, d, i, j, k, B[(color ? npk : 0) + pq], self, use_self != 0, rd);
-    if (omega != T(1)) v = self + omega * (v - self);
-    own[pq] = v;
-}
-
 // FP64 residual of one unknown of (1/dt - Lap) u = b_eff:
 //   r = sum of neighbour terms + b_eff - diag * u,  diag = 1/dt + sum_a c_a/h_a^2
 // with c_a = 2 inside and 1 on a Neumann face (the same rows the sweep solves).
@@ -620,14 +769,11 @@ template <typename T, class R>
 __device__ __forceinline__ double gs_residual_fp64(const GsCoef<T>& c, const Dims& d, int i,
                                                    int j, int k, double b, double u, R r)
 {
-    const double ihx2 = 1.0 / (c.hx * c.hx), ihy2 = 1.0 / (c.hy * c.hy),
-                 ihz2 = 1.0 / (c.hz * c.hz);
     if (!c.neu) {
         const double sx = r(1, 0, 0) + r(-1, 0, 0);
         const double sy = r(0, 1, 0) + r(0, -1, 0);
         const double sz = r(0, 0, 1) + r(0, 0, -1);
-        const double diag = 1.0 / c.dt + 2.0 * ihx2 + 2.0 * ihy2 + 2.0 * ihz2;
-        return sx * ihx2 + sy * ihy2 + sz * ihz2 + b - diag * u;
+        return sx * c.ihx2d + sy * c.ihy2d + sz * c.ihz2d + b - c.diagd * u;
     }
     const int cx = i == 0 ? 0 : (i == d.nx - 1 ? 2 : 1);
     const int cy = j == 0 ? 0 : (j == d.ny - 1 ? 2 : 1);
@@ -640,50 +786,654 @@ __device__ __forceinline__ double gs_residual_fp64(const GsCoef<T>& c, const Dim
                               : (cy == 0 ? r(0, 1, 0) - bcn * c.hy : r(0, -1, 0) + bcn * c.hy);
     const double tz = cz == 1 ? r(0, 0, 1) + r(0, 0, -1)
                               : (cz == 0 ? r(0, 0, 1) - bcn * c.hz : r(0, 0, -1) + bcn * c.hz);
-    const double diag = 1.0 / c.dt + (cx == 1 ? 2.0 : 1.0) * ihx2 + (cy == 1 ? 2.0 : 1.0) * ihy2 +
-                        (cz == 1 ? 2.0 : 1.0) * ihz2;
-    return tx * ihx2 + ty * ihy2 + tz * ihz2 + b - diag * u;
+    const double diag = 1.0 / c.dt + (cx == 1 ? 2.0 : 1.0) * c.ihx2d + (cy == 1 ? 2.0 : 1.0) * c.ihy2d +
+                        (cz == 1 ? 2.0 : 1.0) * c.ihz2d;
+    return tx * c.ihx2d + ty * c.ihy2d + tz * c.ihz2d + b - diag * u;
 }
 
-// Residual of (1/dt - Lap) u = b_eff on the packed layout over the unknowns,
-// accumulated as sum r^2 in FP64 (values read in T, arithmetic in FP64).
-template <typename T>
-__global__ void rb_residual_kernel(const T* __restrict__ U, const T* __restrict__ B, Dims d,
-                                   GsCoef<T> c, double* sums, int want_beff)
+// Red-black half sweep on the packed layout, one thread per packed column (m, j)
+// marching over NI planes of i. The other colour's value at (i, j, m) is the k
+// neighbour on one side of the point of plane i and the i neighbour of the points of
+// planes i-1 and i+1, so a three-deep register window along i serves six of the
+// eight neighbour reads; the other k neighbour is at m-1 (k even) or m+1 (k odd).
+// Interior points take a branch-free path; Neumann boundary points the generic one.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) rb_half_col_kernel(T* __restrict__ U,
+                                                          const T* __restrict__ B, Dims d,
+                                                          GsCoef<T> c, int color, int use_self,
+                                                          T omega)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    double acc = 0, accb = 0;
-    const int lo = c.neu ? 0 : 1;
-    const long long npk = d.npk();
-    if (j < d.ny) {
+    const int i0 = blockIdx.z * NI;
+    const int hz = d.hz();
+    if (m >= hz || j >= d.ny) return;
+    const long long plane = (long long)d.ny * hz;
+    const long long npk = plane * d.nx;
+    T* own = U + (color ? npk : 0);
+    const T* oth = U + (color ? 0 : npk);
+    const T* bb = B + (color ? npk : 0);
+    const bool jint = j >= 1 && j <= d.ny - 2;
+    const long long q0 = ((long long)i0 * d.ny + j) * hz + m;
+    const bool relax = omega != T(1);
+    // all loads of the column first (fixed trip count, predicated), then the updates
+    T o[NI + 2];  // other colour at planes i0-1 .. i0+NI
+    T ys[NI], kn[NI], bv[NI], sf[NI];
 #pragma unroll
-        for (int color = 0; color < 2; ++color) {
-            const int k = 2 * m + ((i + j + color) & 1);
-            if (k >= d.nz) continue;
-            if (i < lo || j < lo || k < lo || i >= d.nx - lo || j >= d.ny - lo || k >= d.nz - lo)
-                continue;
-            const T* own = U + (color ? npk : 0);
-            const T* oth = U + (color ? 0 : npk);
-            const long long pq = d.pidx(i, j, k);
-            auto rd = [&](int oi, int oj, int ok) {
-                return (double)oth[d.pidx(i + oi, j + oj, k + ok)];
-            };
-            const double bv = (double)B[(color ? npk : 0) + pq];
-            const double r = gs_residual_fp64<T>(c, d, i, j, k, bv, (double)own[pq], rd);
-            acc += r * r;
-            accb += bv * bv;
+    for (int t = 0; t < NI + 2; ++t) {
+        const int i = i0 - 1 + t;
+        o[t] = (i >= 0 && i < d.nx) ? oth[q0 + (long long)(t - 1) * plane] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        const long long q = q0 + (long long)t * plane;
+        const int k = 2 * m + ((i + j + color) & 1);
+        const bool in = i >= 1 && i <= d.nx - 2 && jint && k >= 1 && k <= d.nz - 2;
+        ys[t] = in ? oth[q - hz] + oth[q + hz] : T(0);
+        kn[t] = in ? ((k & 1) ? oth[q + 1] : oth[q - 1]) : T(0);
+        bv[t] = in ? bb[q] : T(0);
+        sf[t] = (in && (use_self || relax)) ? own[q] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        if (i >= d.nx) break;
+        const long long q = q0 + (long long)t * plane;
+        const int k = 2 * m + ((i + j + color) & 1);
+        if (k >= d.nz) continue;
+        if (jint && i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2) {
+            const T sz = o[t + 1] + kn[t];
+            const T sy = ys[t];
+            const T sx = o[t] + o[t + 2];
+            const T b = bv[t];
+            const T self = sf[t];
+            T v;
+            if (std::is_same<T, double>::value) {
+                double acc = sx / (c.hx * c.hx) + sy / (c.hy * c.hy) + sz / (c.hz * c.hz) + b;
+                if (use_self) acc = acc + self / c.dt;
+                v = T(acc * (double)c.htilde[7]);
+            } else {
+                T acc = fma(sx, c.ihx2, fma(sy, c.ihy2, fma(sz, c.ihz2, b)));
+                if (use_self) acc = fma(self, c.idt, acc);
+                v = acc * c.htilde[7];
+            }
+            if (relax) v = self + omega * (v - self);
+            own[q] = v;
+        } else if (c.neu) {
+            auto rd = [&](int oi, int oj, int ok) { return oth[d.pidx(i + oi, j + oj, k + ok)]; };
+            const T self = own[q];
+            T v = gs_value<T>(c, d, i, j, k, bb[q], self, use_self != 0, rd);
+            if (relax) v = self + omega * (v - self);
+            own[q] = v;
         }
     }
-    if (want_beff) block_sum2_atomic(acc, accb, sums + SUM_RES2, sums + SUM_BEFF2);
-    else block_sum_atomic(acc, sums + SUM_RES2);
+}
+
+// Vectorised red-black half sweep: one thread per group of W = 16/sizeof(T)
+// consecutive packed points (m0 .. m0+W-1) of row j, marching over NI planes of i.
+// All points of a packed row share the parity of k, so their k neighbours are the
+// other colour at (m-1, m) (k even) or (m, m+1) (k odd): one 16-byte vector plus one
+// scalar. The i neighbours come from a register window of vectors along i.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) rb_half_vec_kernel(T* __restrict__ U,
+                                                          const T* __restrict__ B, Dims d,
+                                                          GsCoef<T> c, int color, int use_self,
+                                                          T omega)
+{
+    typedef V16<T> VT;
+    typedef typename VT::type VV;
+    constexpr int W = VT::W;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    const int hz = d.hz();
+    const int m0 = g * W;
+    if (m0 >= hz || j >= d.ny) return;
+    const long long plane = (long long)d.ny * hz;
+    const long long npk = plane * d.nx;
+    T* own = U + (color ? npk : 0);
+    const T* oth = U + (color ? 0 : npk);
+    const T* bb = B + (color ? npk : 0);
+    const bool jint = j >= 1 && j <= d.ny - 2;
+    const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
+    const bool relax = omega != T(1);
+    VV o[NI + 2];
+#pragma unroll
+    for (int t = 0; t < NI + 2; ++t) {
+        const int i = i0 - 1 + t;
+        if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (long long)(t - 1) * plane);
+        else o[t] = VV{};
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        if (i >= d.nx) break;
+        const long long q = q0 + (long long)t * plane;
+        const int par = (i + j + color) & 1;
+        const bool rowint = jint && i >= 1 && i <= d.nx - 2;
+        if (rowint) {
+            const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
+            const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
+            const VV bv = *reinterpret_cast<const VV*>(bb + q);
+            // the k neighbour not in the centre vector: m0-1 (k even) or m0+W (k odd)
+            const long long qe = par ? q + W : q - 1;
+            const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
+            const T extra = e_ok ? oth[qe] : T(0);
+            VV self = VV{};
+            if (use_self || relax) self = *reinterpret_cast<const VV*>(own + q);
+            VV outv = self;
+            bool all = true;
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                const int k = 2 * (m0 + cc) + par;
+                const bool in = k >= 1 && k <= d.nz - 2;
+                if (!in) {
+                    all = false;
+                    continue;
+                }
+                const T ctr = VT::get(o[t + 1], cc);
+                const T kn = par ? (cc + 1 < W ? VT::get(o[t + 1], cc + 1) : extra)
+                                 : (cc >= 1 ? VT::get(o[t + 1], cc - 1) : extra);
+                const T sz = ctr + kn;
+                const T sy = VT::get(ym, cc) + VT::get(yp, cc);
+                const T sx = VT::get(o[t], cc) + VT::get(o[t + 2], cc);
+                const T b = VT::get(bv, cc);
+                const T sf = VT::get(self, cc);
+                T v;
+                if (std::is_same<T, double>::value) {
+                    double acc = sx / (c.hx * c.hx) + sy / (c.hy * c.hy) + sz / (c.hz * c.hz) + b;
+                    if (use_self) acc = acc + sf / c.dt;
+                    v = T(acc * (double)c.htilde[7]);
+                } else {
+                    T acc = fma(sx, c.ihx2, fma(sy, c.ihy2, fma(sz, c.ihz2, b)));
+                    if (use_self) acc = fma(sf, c.idt, acc);
+                    v = acc * c.htilde[7];
+                }
+                if (relax) v = sf + omega * (v - sf);
+                VT::set(outv, cc, v);
+            }
+            if (all) {
+                *reinterpret_cast<VV*>(own + q) = outv;
+            } else {
+#pragma unroll
+                for (int cc = 0; cc < W; ++cc) {
+                    const int k = 2 * (m0 + cc) + par;
+                    if (k >= 1 && k <= d.nz - 2) own[q + cc] = VT::get(outv, cc);
+                }
+            }
+        }
+        if (c.neu) {
+            // Neumann: boundary points (faces of i, j or k) through the generic rule
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                const int k = 2 * (m0 + cc) + par;
+                if (k >= d.nz) continue;
+                if (rowint && k >= 1 && k <= d.nz - 2) continue;
+                auto rd = [&](int oi, int oj, int ok) { return oth[d.pidx(i + oi, j + oj, k + ok)]; };
+                const T sf = own[q + cc];
+                T v = gs_value<T>(c, d, i, j, k, bb[q + cc], sf, use_self != 0, rd);
+                if (relax) v = sf + omega * (v - sf);
+                own[q + cc] = v;
+            }
+        }
+    }
+}
+
+// Vectorised FP64 residual, same walk as rb_half_vec_kernel; blockIdx.z covers
+// (plane block, colour).
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restrict__ U,
+                                                              const T* __restrict__ B, Dims d,
+                                                              GsCoef<T> c, double* part,
+                                                              int want_beff)
+{
+    typedef V16<T> VT;
+    typedef typename VT::type VV;
+    constexpr int W = VT::W;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int color = blockIdx.z & 1;
+    const int i0 = (blockIdx.z >> 1) * NI;
+    const int hz = d.hz();
+    const int m0 = g * W;
+    double acc = 0, accb = 0;
+    if (m0 < hz && j < d.ny) {
+        const long long plane = (long long)d.ny * hz;
+        const long long npk = plane * d.nx;
+        const T* own = U + (color ? npk : 0);
+        const T* oth = U + (color ? 0 : npk);
+        const T* bb = B + (color ? npk : 0);
+        const bool jint = j >= 1 && j <= d.ny - 2;
+        const int lo = c.neu ? 0 : 1;
+        const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
+        VV o[NI + 2];
+#pragma unroll
+        for (int t = 0; t < NI + 2; ++t) {
+            const int i = i0 - 1 + t;
+            if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (long long)(t - 1) * plane);
+            else o[t] = VV{};
+        }
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            const int i = i0 + t;
+            if (i >= d.nx) break;
+            const long long q = q0 + (long long)t * plane;
+            const int par = (i + j + color) & 1;
+            const bool rowint = jint && i >= 1 && i <= d.nx - 2;
+            const VV bv = *reinterpret_cast<const VV*>(bb + q);
+            const VV uv = *reinterpret_cast<const VV*>(own + q);
+            if (rowint) {
+                const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
+                const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
+                const long long qe = par ? q + W : q - 1;
+                const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
+                const double extra = e_ok ? (double)oth[qe] : 0.0;
+#pragma unroll
+                for (int cc = 0; cc < W; ++cc) {
+                    const int k = 2 * (m0 + cc) + par;
+                    if (!(k >= 1 && k <= d.nz - 2)) continue;
+                    const double ctr = (double)VT::get(o[t + 1], cc);
+                    const double kn = par ? (cc + 1 < W ? (double)VT::get(o[t + 1], cc + 1) : extra)
+                                          : (cc >= 1 ? (double)VT::get(o[t + 1], cc - 1) : extra);
+                    const double b = (double)VT::get(bv, cc);
+                    const double r = ((double)VT::get(o[t], cc) + (double)VT::get(o[t + 2], cc)) * c.ihx2d +
+                                     ((double)VT::get(ym, cc) + (double)VT::get(yp, cc)) * c.ihy2d +
+                                     (ctr + kn) * c.ihz2d + b - c.diagd * (double)VT::get(uv, cc);
+                    acc += r * r;
+                    accb += b * b;
+                }
+            }
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                const int k = 2 * (m0 + cc) + par;
+                if (k >= d.nz) continue;
+                if (rowint && k >= 1 && k <= d.nz - 2) continue;
+                if (!(i >= lo && j >= lo && k >= lo && i < d.nx - lo && j < d.ny - lo && k < d.nz - lo))
+                    continue;
+                auto rd = [&](int oi, int oj, int ok) {
+                    return (double)oth[d.pidx(i + oi, j + oj, k + ok)];
+                };
+                const double b = (double)VT::get(bv, cc);
+                const double r = gs_residual_fp64<T>(c, d, i, j, k, b, (double)VT::get(uv, cc), rd);
+                acc += r * r;
+                accb += b * b;
+            }
+        }
+    }
+    if (want_beff) block_sum2_store(acc, accb, part);
+    else block_sum_store(acc, part);
+}
+
+// FP64 residual of (1/dt - Lap) u = b_eff on the packed layout, same column walk;
+// blockIdx.z covers (plane block, colour). Accumulates sum r^2 and, when asked,
+// sum b_eff^2 over the unknowns.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) rb_residual_col_kernel(const T* __restrict__ U,
+                                                              const T* __restrict__ B, Dims d,
+                                                              GsCoef<T> c, double* part,
+                                                              int want_beff)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int color = blockIdx.z & 1;
+    const int i0 = (blockIdx.z >> 1) * NI;
+    const int hz = d.hz();
+    double acc = 0, accb = 0;
+    if (m < hz && j < d.ny) {
+        const long long plane = (long long)d.ny * hz;
+        const long long npk = plane * d.nx;
+        const T* own = U + (color ? npk : 0);
+        const T* oth = U + (color ? 0 : npk);
+        const T* bb = B + (color ? npk : 0);
+        const bool jint = j >= 1 && j <= d.ny - 2;
+        const int lo = c.neu ? 0 : 1;
+        const long long q0 = ((long long)i0 * d.ny + j) * hz + m;
+        double o[NI + 2];
+#pragma unroll
+        for (int t = 0; t < NI + 2; ++t) {
+            const int i = i0 - 1 + t;
+            o[t] = (i >= 0 && i < d.nx) ? (double)oth[q0 + (long long)(t - 1) * plane] : 0.0;
+        }
+        double ys[NI], kn[NI], bv[NI], uv[NI];
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            const int i = i0 + t;
+            const long long q = q0 + (long long)t * plane;
+            const int k = 2 * m + ((i + j + color) & 1);
+            const bool in = i >= 1 && i <= d.nx - 2 && jint && k >= 1 && k <= d.nz - 2;
+            const bool any = i < d.nx && k < d.nz;
+            ys[t] = in ? (double)oth[q - hz] + (double)oth[q + hz] : 0.0;
+            kn[t] = in ? ((k & 1) ? (double)oth[q + 1] : (double)oth[q - 1]) : 0.0;
+            bv[t] = any ? (double)bb[q] : 0.0;
+            uv[t] = any ? (double)own[q] : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            const int i = i0 + t;
+            if (i >= d.nx) break;
+            const long long q = q0 + (long long)t * plane;
+            const int k = 2 * m + ((i + j + color) & 1);
+            if (k >= d.nz) continue;
+            if (jint && i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2) {
+                const double r = (o[t] + o[t + 2]) * c.ihx2d + ys[t] * c.ihy2d +
+                                 (o[t + 1] + kn[t]) * c.ihz2d + bv[t] - c.diagd * uv[t];
+                acc += r * r;
+                accb += bv[t] * bv[t];
+            } else if (i >= lo && j >= lo && k >= lo && i < d.nx - lo && j < d.ny - lo &&
+                       k < d.nz - lo) {
+                auto rd = [&](int oi, int oj, int ok) {
+                    return (double)oth[d.pidx(i + oi, j + oj, k + ok)];
+                };
+                const double r = gs_residual_fp64<T>(c, d, i, j, k, bv[t], uv[t], rd);
+                acc += r * r;
+                accb += bv[t] * bv[t];
+            }
+        }
+    }
+    if (want_beff) block_sum2_store(acc, accb, part);
+    else block_sum_store(acc, part);
+}
+
+// cut_phi (rsfe_splitbregman_imp.hxx:320-339) and the tolerance sums of :1832:
+// phi holds phiold on entry and the clamped solve result on exit (natural layout);
+// u is the solve result (packed or natural); u_out, when given, receives it unclamped.
+template <typename T, bool PACKED, int NI>
+__global__ void __launch_bounds__(256) clamp_tol_kernel(const T* __restrict__ u, T* phi,
+                                                        T* __restrict__ u_out, Dims d, T a0, T b0,
+                                                        double* part)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    double s_d = 0, s_o = 0;
+    if (k < d.nz && j < d.ny) {
+        const int i_end = min(i0 + NI, d.nx);
+        const long long plane = (long long)d.ny * d.nz;
+        const long long pplane = (long long)d.ny * d.hz();
+        long long p = d.idx(i0, j, k);
+        long long pq = d.pidx(i0, j, k);
+        const long long npk = pplane * d.nx;
+        for (int i = i0; i < i_end; ++i, p += plane, pq += pplane) {
+            const T uv = PACKED ? u[pq + (((i + j + k) & 1) ? npk : 0)] : u[p];
+            if (u_out) u_out[p] = uv;
+            T v = uv;
+            if (v < a0) v = a0;
+            else if (v > b0) v = b0;
+            const T old = phi[p];
+            phi[p] = v;
+            const double df = (double)v - (double)old;
+            s_d += df * df;
+            s_o += (double)old * (double)old;
+        }
+    }
+    block_sum2_store(s_d, s_o, part);
+}
+
+// The Split-Bregman update on the clamped phi (rsfe_splitbregman_imp.hxx:1868-1906),
+// per component c: d = grad(phi)_c; b += d; d = shrink(b, g); b -= d; d -= b.
+// Thread per (k, j) column marching over NI planes with phi(i-1), phi(i), phi(i+1)
+// in registers; j and k neighbours come through L1.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
+                                                      T* __restrict__ b3, T* __restrict__ dmb,
+                                                      const T* __restrict__ g, Dims d, double hx,
+                                                      double hy, double hz)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    if (k >= d.nz || j >= d.ny) return;
+    const int i_end = min(i0 + NI, d.nx);
+    const long long plane = (long long)d.ny * d.nz;
+    const long long n = d.n();
+    const long long sy = d.nz;
+    long long p = d.idx(i0, j, k);
+    T fm = i0 >= 1 ? phi[p - plane] : T(0);
+    T f0 = phi[p];
+    const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    for (int i = i0; i < i_end; ++i, p += plane) {
+        const T fp = i + 1 < d.nx ? phi[p + plane] : T(0);
+        T gr[3];
+        if (i == 0) gr[0] = (T(4) * fp - T(3) * f0 - phi[p + 2 * plane]) / two_hx;
+        else if (i == d.nx - 1) gr[0] = (T(3) * f0 - T(4) * fm + phi[p - 2 * plane]) / two_hx;
+        else gr[0] = (fp - fm) / two_hx;
+        if (j == 0) gr[1] = (T(4) * phi[p + sy] - T(3) * f0 - phi[p + 2 * sy]) / two_hy;
+        else if (j == d.ny - 1) gr[1] = (T(3) * f0 - T(4) * phi[p - sy] + phi[p - 2 * sy]) / two_hy;
+        else gr[1] = (phi[p + sy] - phi[p - sy]) / two_hy;
+        if (k == 0) gr[2] = (T(4) * phi[p + 1] - T(3) * f0 - phi[p + 2]) / two_hz;
+        else if (k == d.nz - 1) gr[2] = (T(3) * f0 - T(4) * phi[p - 1] + phi[p - 2]) / two_hz;
+        else gr[2] = (phi[p + 1] - phi[p - 1]) / two_hz;
+        const T gg = g[p];
+#pragma unroll
+        for (int cmp = 0; cmp < 3; ++cmp) {
+            T bv = b3[cmp * n + p];
+            bv += gr[cmp];
+            const T mag = fabs(bv) - gg;
+            const T sgn = T((int)(bv > T(0)) - (int)(bv < T(0)));
+            const T dn = sgn * ((mag < T(0)) ? T(0) : mag);
+            bv -= dn;
+            b3[cmp * n + p] = bv;
+            dmb[cmp * n + p] = dn - bv;
+        }
+        fm = f0;
+        f0 = fp;
+    }
+}
+
+// ---- vectorised natural-layout kernels (nz a multiple of W = 16/sizeof(T)) ----
+// Thread per group of W consecutive k of row j, marching over NI planes of i.
+
+// cut_phi + tolerance sums, reading the solve result from the packed layout: for
+// natural k = kb .. kb+W-1 (kb even) the even k sit in the colour array of (i+j)&1 and
+// the odd k in the other, both at m = kb/2 .. kb/2 + W/2 - 1.
+template <typename T, bool PACKED, int NI>
+__global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict__ u, T* phi,
+                                                            T* __restrict__ u_out, Dims d, T a0,
+                                                            T b0, double* part)
+{
+    typedef V16<T> VT;
+    typedef typename VT::type VV;
+    constexpr int W = VT::W;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    const int kb = g * W;
+    double s_d = 0, s_o = 0;
+    if (kb < d.nz && j < d.ny) {
+        const long long plane = (long long)d.ny * d.nz;
+        const long long pplane = (long long)d.ny * d.hz();
+        const long long npk = pplane * d.nx;
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            const int i = i0 + t;
+            if (i >= d.nx) break;
+            const long long p = d.idx(i, j, kb);
+            VV uv;
+            if (PACKED) {
+                const long long pq = ((long long)i * d.ny + j) * d.hz() + (kb >> 1);
+                const int c0 = (i + j) & 1;  // colour of the even k
+                const T* ev = u + (c0 ? npk : 0) + pq;
+                const T* od = u + (c0 ? 0 : npk) + pq;
+#pragma unroll
+                for (int h = 0; h < W / 2; ++h) {
+                    VT::set(uv, 2 * h, ev[h]);
+                    VT::set(uv, 2 * h + 1, od[h]);
+                }
+            } else {
+                uv = *reinterpret_cast<const VV*>(u + p);
+            }
+            if (u_out) *reinterpret_cast<VV*>(u_out + p) = uv;
+            const VV old = *reinterpret_cast<const VV*>(phi + p);
+            VV nv;
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                T v = VT::get(uv, cc);
+                if (v < a0) v = a0;
+                else if (v > b0) v = b0;
+                VT::set(nv, cc, v);
+                const double o = (double)VT::get(old, cc);
+                const double df = (double)v - o;
+                s_d += df * df;
+                s_o += o * o;
+            }
+            *reinterpret_cast<VV*>(phi + p) = nv;
+        }
+    }
+    block_sum2_store(s_d, s_o, part);
+}
+
+// Split-Bregman update (see bregman_kernel), vectorised along k; points on a face of
+// the volume take the scalar one-sided stencils.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ phi,
+                                                          T* __restrict__ b3, T* __restrict__ dmb,
+                                                          const T* __restrict__ g3, Dims d,
+                                                          double hx, double hy, double hz)
+{
+    typedef V16<T> VT;
+    typedef typename VT::type VV;
+    constexpr int W = VT::W;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    const int kb = g * W;
+    if (kb >= d.nz || j >= d.ny) return;
+    const long long plane = (long long)d.ny * d.nz;
+    const long long sy = d.nz;
+    const long long n = d.n();
+    const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    const bool jint = j >= 1 && j <= d.ny - 2;
+    const long long p0 = d.idx(i0, j, kb);
+    VV f[NI + 2];
+#pragma unroll
+    for (int t = 0; t < NI + 2; ++t) {
+        const int i = i0 - 1 + t;
+        if (i >= 0 && i < d.nx) f[t] = *reinterpret_cast<const VV*>(phi + p0 + (long long)(t - 1) * plane);
+        else f[t] = VV{};
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        if (i >= d.nx) break;
+        const long long p = p0 + (long long)t * plane;
+        const bool rowint = jint && i >= 1 && i <= d.nx - 2;
+        VV ym = VV{}, yp = VV{};
+        if (rowint) {
+            ym = *reinterpret_cast<const VV*>(phi + p - sy);
+            yp = *reinterpret_cast<const VV*>(phi + p + sy);
+        }
+        const T km = kb >= 1 ? phi[p - 1] : T(0);
+        const T kp = kb + W < d.nz ? phi[p + W] : T(0);
+        const VV gg = *reinterpret_cast<const VV*>(g3 + p);
+        VV bo[3], dn[3];
+#pragma unroll
+        for (int cmp = 0; cmp < 3; ++cmp) bo[cmp] = *reinterpret_cast<const VV*>(b3 + cmp * n + p);
+#pragma unroll
+        for (int cc = 0; cc < W; ++cc) {
+            const int k = kb + cc;
+            T gr[3];
+            if (rowint && k >= 1 && k <= d.nz - 2) {
+                gr[0] = (VT::get(f[t + 2], cc) - VT::get(f[t], cc)) / two_hx;
+                gr[1] = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
+                const T fkp = cc + 1 < W ? VT::get(f[t + 1], cc + 1) : kp;
+                const T fkm = cc >= 1 ? VT::get(f[t + 1], cc - 1) : km;
+                gr[2] = (fkp - fkm) / two_hz;
+            } else {
+                const long long pc = p + cc;
+                gr[0] = grad_term(phi, pc, plane, i, d.nx, hx);
+                gr[1] = grad_term(phi, pc, sy, j, d.ny, hy);
+                gr[2] = grad_term(phi, pc, 1, k, d.nz, hz);
+            }
+            const T gv = VT::get(gg, cc);
+#pragma unroll
+            for (int cmp = 0; cmp < 3; ++cmp) {
+                T bv = VT::get(bo[cmp], cc);
+                bv += gr[cmp];
+                const T mag = fabs(bv) - gv;
+                const T sgn = T((int)(bv > T(0)) - (int)(bv < T(0)));
+                const T dd = sgn * ((mag < T(0)) ? T(0) : mag);
+                bv -= dd;
+                VT::set(bo[cmp], cc, bv);
+                VT::set(dn[cmp], cc, dd - bv);
+            }
+        }
+#pragma unroll
+        for (int cmp = 0; cmp < 3; ++cmp) {
+            *reinterpret_cast<VV*>(b3 + cmp * n + p) = bo[cmp];
+            *reinterpret_cast<VV*>(dmb + cmp * n + p) = dn[cmp];
+        }
+    }
+}
+
+// im3d::div vectorised along k (see div_point); points on a face of the volume take
+// the scalar rule with the reference's quirks.
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T* __restrict__ out,
+                                                      Dims d, double hx, double hy, double hz)
+{
+    typedef V16<T> VT;
+    typedef typename VT::type VV;
+    constexpr int W = VT::W;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = blockIdx.z * NI;
+    const int kb = g * W;
+    if (kb >= d.nz || j >= d.ny) return;
+    const long long plane = (long long)d.ny * d.nz;
+    const long long sy = d.nz;
+    const long long n = d.n();
+    const T* f0 = v;
+    const T* f1 = v + n;
+    const T* f2 = v + 2 * n;
+    const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    const bool jint = j >= 1 && j <= d.ny - 2;
+    const long long p0 = d.idx(i0, j, kb);
+    VV x[NI + 2];
+#pragma unroll
+    for (int t = 0; t < NI + 2; ++t) {
+        const int i = i0 - 1 + t;
+        if (i >= 0 && i < d.nx) x[t] = *reinterpret_cast<const VV*>(f0 + p0 + (long long)(t - 1) * plane);
+        else x[t] = VV{};
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        if (i >= d.nx) break;
+        const long long p = p0 + (long long)t * plane;
+        const bool rowint = jint && i >= 1 && i <= d.nx - 2;
+        VV o;
+        if (rowint) {
+            const VV ym = *reinterpret_cast<const VV*>(f1 + p - sy);
+            const VV yp = *reinterpret_cast<const VV*>(f1 + p + sy);
+            const VV zc = *reinterpret_cast<const VV*>(f2 + p);
+            const T km = kb >= 1 ? f2[p - 1] : T(0);
+            const T kp = kb + W < d.nz ? f2[p + W] : T(0);
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) {
+                const int k = kb + cc;
+                if (k >= 1 && k <= d.nz - 2) {
+                    const T tx = (VT::get(x[t + 2], cc) - VT::get(x[t], cc)) / two_hx;
+                    const T ty = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
+                    const T zp = cc + 1 < W ? VT::get(zc, cc + 1) : kp;
+                    const T zm = cc >= 1 ? VT::get(zc, cc - 1) : km;
+                    VT::set(o, cc, tx + ty + (zp - zm) / two_hz);
+                } else {
+                    VT::set(o, cc, div_point(f0, f1, f2, d, i, j, k, hx, hy, hz));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int cc = 0; cc < W; ++cc) VT::set(o, cc, div_point(f0, f1, f2, d, i, j, kb + cc, hx, hy, hz));
+        }
+        *reinterpret_cast<VV*>(out + p) = o;
+    }
 }
 
 // sum (a - b)^2 and sum b^2 over n elements (relative change of a sweep)
 template <typename T>
 __global__ void diff_sums_kernel(const T* __restrict__ a, const T* __restrict__ b, long long n,
-                                 double* sums)
+                                 double* part)
 {
     double sd = 0, sb = 0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
@@ -692,7 +1442,7 @@ __global__ void diff_sums_kernel(const T* __restrict__ a, const T* __restrict__ 
         sd += x * x;
         sb += (double)b[q] * (double)b[q];
     }
-    block_sum2_atomic(sd, sb, sums + SUM_A, sums + SUM_B);
+    block_sum2_store(sd, sb, part);
 }
 
 // natural -> packed copy of a volume (both colours), and back
@@ -719,7 +1469,7 @@ __global__ void unpack_kernel(const T* __restrict__ src, T* __restrict__ dst, Di
 // packed b_eff = b + u/dt (u packed), with sum b_eff^2; Dirichlet faces of u := bc
 template <typename T>
 __global__ void make_beff_kernel(const T* __restrict__ b, T* __restrict__ U, T* __restrict__ Beff,
-                                 Dims d, T inv_dt, T bc, int dirichlet, double* sums)
+                                 Dims d, T inv_dt, T bc, int dirichlet, double* part)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -738,7 +1488,7 @@ __global__ void make_beff_kernel(const T* __restrict__ b, T* __restrict__ U, T* 
         Beff[pq] = e;
         if (!(dirichlet && face)) acc = (double)e * (double)e;
     }
-    block_sum_atomic(acc, sums + SUM_BEFF2);
+    if (part) block_sum_store(acc, part);
 }
 
 // ------------------------------------------------------------------ utilities

@@ -40,7 +40,7 @@ UNIT = "Gvoxel-iters/s"
 SHAPE = (256, 256, 256)
 MAXITER = 100
 PARAMS = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, dt=1.0, a0=0.0,
-              b0=1.0, bc=2, maxiter=MAXITER, tol=0.0, gs_rel_res_tol=1e-6, gs_check_every=2,
+              b0=1.0, bc=2, maxiter=MAXITER, tol=0.0, gs_rel_res_tol=1e-6, gs_check_every=0,
               gs_max_sweeps=1000, omega=1.0)
 
 # Algorithmic bytes per voxel of one launch of each loop kernel (FP32): the

@@ -82,7 +82,8 @@ typedef struct im3d_rsfe_params {
     int32_t init_variables;     /* reset b and div(d-b) after the first iteration (0) */
     int32_t sweep;              /* IM3D_SWEEP_* used by the ls_steps sweeps (LEXICOGRAPHIC) */
     int32_t gs_max_sweeps;      /* sweep cap of the residual solve (1000) */
-    int32_t gs_check_every;     /* residual evaluated every this many sweeps (2) */
+    int32_t gs_check_every;     /* residual every this many sweeps; 0 = predicted from the
+                                   observed contraction rate (0) */
 } im3d_rsfe_params;
 
 typedef struct im3d_rsfe_stats {

@@ -315,9 +315,24 @@ static void solve_residual(const gs_geom* g, const double* u, const double* uin,
     *bb = sb;
 }
 
+/* Next residual check: a fixed interval when check_every > 0; otherwise first
+ * checks after 4 and 8 sweeps, then ceil(log(tol/r_s)/log(rate)) sweeps later with
+ * rate = (r_s/r_prev)^(1/(s - s_prev)), clamped to [1, 32]. */
+static int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every)
+{
+    if (check_every > 0) return s + check_every;
+    if (s_prev <= 0 || !(r_prev > r_s) || !(r_s > 0)) return s + 4;
+    double rate = pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    double need = log(tol / r_s) / log(rate);
+    int step = 32;
+    if (need == need && need < 32.0) step = (int)ceil(need);
+    if (step < 1) step = 1;
+    return s + step;
+}
+
 /* Red-black solve of (1/dt - Lap) u = uin/dt + b with uin = u on entry held fixed
  * (the converged form of one unsteady step; the reference's single sweep is its
- * first Gauss-Seidel iterate). Residual checked every check_every sweeps. */
+ * first Gauss-Seidel iterate). Residual checked on the schedule of next_check. */
 int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double hx, double hy,
                       double hz, double dt, double bc, int bc_type, double rel_res_tol,
                       int max_sweeps, int check_every, double omega, int* sweeps_done,
@@ -331,9 +346,11 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
     memcpy(uin, u, n * sizeof(double));
     int lo = g.neu ? 0 : 1;
     int hix = g.neu ? nx : nx - 1, hiy = g.neu ? ny : ny - 1, hiz = g.neu ? nz : nz - 1;
-    if (check_every < 1) check_every = 1;
-    int s = 0, conv = 0;
-    double rel = -1;
+    if (check_every < 0) check_every = 0;
+    if (max_sweeps < 1) max_sweeps = 1;
+    int s = 0, conv = 0, s_prev = 0;
+    int next = check_every > 0 ? check_every : 4;
+    double rel = -1, r_prev = -1;
     while (s < max_sweeps) {
         for (int color = 0; color < 2; ++color) {
             #pragma omp parallel for schedule(static)
@@ -348,11 +365,15 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
             }
         }
         ++s;
-        if (s % check_every == 0 || s == max_sweeps) {
+        if (s >= next || s == max_sweeps) {
             double rr, bb;
             solve_residual(&g, u, uin, b, &rr, &bb);
             rel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
             if (rel <= rel_res_tol) { conv = 1; break; }
+            next = next_check(s, rel, s_prev, r_prev, rel_res_tol, check_every);
+            if (next > max_sweeps) next = max_sweeps;
+            s_prev = s;
+            r_prev = rel;
         }
     }
     free(uin);

@@ -59,7 +59,7 @@ def default_params(**kw) -> RsfeParams:
                    nu=1.0, dt=1.0, epsilon=1e-3, a0=0.0, b0=1.0, ls_tol=0.0,
                    edge_detector_sigma=0.0, gs_rel_res_tol=0.0, omega=1.0, maxiter=100,
                    ls_steps=5, bc=BC_DEFAULT, gaussian_pixel_approach=0, init_variables=0,
-                   sweep=SWEEP_LEX, gs_max_sweeps=1000, gs_check_every=2)
+                   sweep=SWEEP_LEX, gs_max_sweeps=1000, gs_check_every=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -141,7 +141,7 @@ def poisson_sweeps(res, b, dt=1.0, bc=0.0, bc_type=BC_DIR, order=SWEEP_LEX, swee
 
 
 def poisson_solve(u, b, dt=1.0, bc=0.0, bc_type=BC_DIR, tol=1e-6, max_sweeps=1000,
-                  check_every=2, omega=1.0, h=(1.0, 1.0, 1.0)):
+                  check_every=0, omega=1.0, h=(1.0, 1.0, 1.0)):
     u = _f64(u).copy()
     b = _f64(b)
     sw = C.c_int(0)

@@ -57,7 +57,7 @@ struct Recorder
     int mode = 0;     // 0 reference Dir, 1 reference Neu, 2 red-black sweep, 3 residual solve
     int bc_type = IM3D_BC_DIR;
     double rel_res_tol = 0, omega = 1;
-    int max_sweeps = 1000, check_every = 2;
+    int max_sweeps = 1000, check_every = 0;
     long long sweeps = 0;
     int last_sweeps = 0;
     double last_rel = -1;
