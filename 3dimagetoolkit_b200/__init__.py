@@ -10,7 +10,7 @@ The package name starts with a digit, so import it with
 """
 from ._abi import (BC_DEFAULT, BC_DIR, BC_NEU, SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK, Context,
                    Im3dError, RsfeParams, RsfeStats, default_params, lib)
-from . import synth
+from . import mhd, synth
 
-__all__ = ["Context", "Im3dError", "RsfeParams", "RsfeStats", "default_params", "lib", "synth",
+__all__ = ["Context", "Im3dError", "RsfeParams", "RsfeStats", "default_params", "lib", "mhd", "synth",
            "BC_DEFAULT", "BC_DIR", "BC_NEU", "SWEEP_LEXICOGRAPHIC", "SWEEP_REDBLACK"]

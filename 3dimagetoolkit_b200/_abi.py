@@ -72,6 +72,14 @@ class RsfeStats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
+class VolumeDesc(C.Structure):
+    """``im3d_volume_desc``: one volume of a batch."""
+
+    _fields_ = [("myim", C.c_void_p), ("init", C.c_void_p), ("phi_out", C.c_void_p),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("reserved", C.c_int32),
+                ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double)]
+
+
 _lib = None
 
 
@@ -254,6 +262,28 @@ class Context:
                             C.c_int(max_sweeps), C.c_int(check_every), C.c_double(omega),
                             C.byref(sw), C.byref(rel)), allow=(ERR_NOT_CONVERGED,))
         return int(sw.value), float(rel.value), st == OK
+
+    def rsfe_apply_batched(self, volumes, inits=None, params: RsfeParams | None = None,
+                           streams: int = 4, outs=None, h=(1.0, 1.0, 1.0)):
+        """Segments a list of volumes (same dtype); returns (phis, stats, latency_ms)."""
+        p = params if params is not None else default_params()
+        n = len(volumes)
+        inits = inits if inits is not None else [None] * n
+        outs = outs if outs is not None else [_empty_like(v) for v in volumes]
+        descs = (VolumeDesc * n)()
+        dt = None
+        for q, (v, i0, o) in enumerate(zip(volumes, inits, outs)):
+            pv, dt = _ptr(v)
+            descs[q].myim = pv
+            descs[q].init = _ptr(i0)[0]
+            descs[q].phi_out = _ptr(o)[0]
+            descs[q].nx, descs[q].ny, descs[q].nz = (int(s) for s in v.shape)
+            descs[q].hx, descs[q].hy, descs[q].hz = h
+        stats = (RsfeStats * n)()
+        lat = (C.c_double * n)()
+        fn = getattr(lib(), "im3d_rsfe_apply_batched_" + _suffix(dt))
+        self._check(fn(self._h, C.c_int(n), descs, C.byref(p), C.c_int(streams), stats, lat))
+        return outs, [s.as_dict() for s in stats], list(lat)
 
     def rsfe_apply(self, myim, init=None, params: RsfeParams | None = None, h=(1.0, 1.0, 1.0),
                    want_u=False, want_f=False, phi_out=None):

@@ -32,7 +32,12 @@ __device__ __forceinline__ void heaviside_pair(T phi, T center, T inv_eps, T& H,
     const T x = (phi - center) * inv_eps;
     const T y = fabs(x);
     T small;
-    if (y >= T(1)) small = atan(T(1) / y) * inv_pi;
+    if (y >= T(1)) {
+        T inv_y;
+        if constexpr (sizeof(T) == 4) inv_y = __frcp_rn(y);  // = 1.0f / y, correctly rounded
+        else inv_y = T(1) / y;
+        small = atan(inv_y) * inv_pi;
+    }
     else small = T(0.5) - atan(y) * inv_pi;
     const T large = T(1) - small;
     if (x > T(0)) { H = large; Hb = small; }
@@ -313,36 +318,42 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     load_taps<T, S>(taps, w);
     __syncthreads();
     const int kk = k0 + threadIdx.x * R;
-    if (!live || kk >= d.nz) return;
-    Vec<T, N> out[R];
+    const bool act = live && kk < d.nz;
+    T res[N][R];
+    if (act) {
 #pragma unroll
-    for (int q = 0; q < N; ++q) {
-        const T* base = sm + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
-        T xa[XW];
-        if (sizeof(T) == 4) {
+        for (int q = 0; q < N; ++q) {
+            const T* base = sm + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
+            T xa[XW];
+            if (sizeof(T) == 4) {
 #pragma unroll
-            for (int t = 0; t < XW; t += 4) {
-                const float4 v4 = *reinterpret_cast<const float4*>(base + t);
-                xa[t] = v4.x; xa[t + 1] = v4.y; xa[t + 2] = v4.z; xa[t + 3] = v4.w;
+                for (int t = 0; t < XW; t += 4) {
+                    const float4 v4 = *reinterpret_cast<const float4*>(base + t);
+                    xa[t] = v4.x; xa[t + 1] = v4.y; xa[t + 2] = v4.z; xa[t + 3] = v4.w;
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < XW; t += 2) {
+                    const double2 v2 = *reinterpret_cast<const double2*>(base + t);
+                    xa[t] = v2.x; xa[t + 1] = v2.y;
+                }
             }
-        } else {
+            T x[R + 2 * S];
 #pragma unroll
-            for (int t = 0; t < XW; t += 2) {
-                const double2 v2 = *reinterpret_cast<const double2*>(base + t);
-                xa[t] = v2.x; xa[t + 1] = v2.y;
-            }
+            for (int t = 0; t < R + 2 * S; ++t) x[t] = xa[t + SP - S];
+            window_conv<T, S, R>(x, w, res[q]);
         }
-        T x[R + 2 * S];
-#pragma unroll
-        for (int t = 0; t < R + 2 * S; ++t) x[t] = xa[t + SP - S];
-        T o[R];
-        window_conv<T, S, R>(x, w, o);
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[r].v[q] = o[r];
     }
+    if (!act) return;
 #pragma unroll
-    for (int r = 0; r < R; ++r)
-        if (kk + r < d.nz) st(i, j, kk + r, out[r]);
+    for (int r = 0; r < R; ++r) {
+        if (kk + r < d.nz) {
+            Vec<T, N> v;
+#pragma unroll
+            for (int q = 0; q < N; ++q) v.v[q] = res[q][r];
+            st(i, j, kk + r, v);
+        }
+    }
 }
 
 // Along j (AXIS 1) or i (AXIS 0). Block TW x TY; each thread R consecutive outputs

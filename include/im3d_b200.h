@@ -202,6 +202,31 @@ int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, i
                         double* phi_out, double* u_out, double* f1_out, double* f2_out,
                         im3d_rsfe_stats* stats);
 
+/* A batch of independent volumes (BASELINE's uneven-volume workload). No counterpart
+ * in the reference, which segments one image per apply(). Each descriptor holds the
+ * caller's buffers (host or device, T = float for _f32, double for _f64), the size
+ * and the spacing. */
+typedef struct im3d_volume_desc {
+    const void* myim;   /* image to segment */
+    const void* init;   /* initial level set, NULL = the default cube */
+    void* phi_out;      /* receives getoutput() */
+    int32_t nx, ny, nz, reserved;
+    double hx, hy, hz;
+} im3d_volume_desc;
+
+/* Segments nvol volumes with the same parameters. Volumes are taken largest first from
+ * a shared queue by `streams` workers (0 = 4), each running whole segmentations on
+ * its own CUDA stream with its own device buffers, so small volumes overlap on the
+ * GPU. stats and latency_ms (either may be NULL) receive nvol entries: the statistics
+ * of each volume and the time from the start of the call to that volume's result.
+ * Returns the first non-OK status (the other volumes still run). */
+int im3d_rsfe_apply_batched_f32(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
+                                const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
+                                double* latency_ms);
+int im3d_rsfe_apply_batched_f64(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
+                                const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
+                                double* latency_ms);
+
 #ifdef __cplusplus
 }
 #endif
