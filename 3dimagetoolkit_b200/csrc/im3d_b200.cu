@@ -59,6 +59,8 @@ struct im3d_ctx {
     size_t persist_max = 0;
     size_t window_max = 0;
     bool persist_set = false;
+    // temporally blocked sweep pairs for FP32 solves (opt-in: IM3D_TB=1)
+    bool tb_enabled = false;
 };
 
 namespace {
@@ -650,6 +652,30 @@ void l2_unpin(im3d_ctx* ctx)
     if (cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
 }
 
+// Two red-black sweeps in one temporally blocked pass (rb_tb2_kernel), optionally
+// with the FP64 residual of the result (want_res 1) and sum b_eff^2 (want_res 2)
+// folded into ctrl->sum[SUM_RES2 ..].
+constexpr int kTbJ = 16, kTbM = 32, kTbI = 32;
+
+template <typename T>
+int rb_tb_pass(im3d_ctx* ctx, const T* Uin, T* Uout, const T* B, const Dims& d, const GsCoef<T>& c,
+               int want_res)
+{
+    constexpr int H = TbRing<T>::H, NP = TbRing<T>::NP;
+    const size_t smem = (size_t)NP * 2 * (kTbJ + 2 * H) * (kTbM + 2 * H) * sizeof(T);
+    auto kern = rb_tb2_kernel<T, kTbJ, kTbM, kTbI>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    const dim3 grid((d.hz() + kTbM - 1) / kTbM, (d.ny + kTbJ - 1) / kTbJ, (d.nx + kTbI - 1) / kTbI);
+    double* part = nullptr;
+    if (want_res) IM3D_TRY(part_buf(ctx, grid, want_res == 2 ? 2 : 1, &part));
+    const int pf = prof_begin(ctx, "rb_tb2");
+    kern<<<grid, 256, smem, ctx->stream>>>(Uin, Uout, B, d, c, part, want_res);
+    prof_end(ctx, pf);
+    IM3D_TRY(check_launch(ctx, "rb_tb2"));
+    if (want_res) IM3D_TRY(finalize(ctx, part, grid, want_res == 2 ? 2 : 1, SUM_RES2));
+    return IM3D_OK;
+}
+
 // Red-black solve on the packed layout (U holds u_in on entry, B = b_eff packed).
 // Residual every check_every sweeps; sum b_eff^2 is taken on the first check.
 template <typename T>
@@ -669,6 +695,45 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
         im3d_ctx* c;
         ~Unpin() { l2_unpin(c); }
     } unpin{ctx};
+    // FP32 with omega == 1: sweeps go in temporally blocked pairs, and the residual
+    // of a pair comes out of the same pass; checks land on pair boundaries
+    const bool tb = sizeof(T) == 4 && omega == 1.0 && ctx->tb_enabled && max_sweeps >= 2;
+    if (tb) {
+        // passes alternate between U and a second packed buffer
+        const size_t cnt = 2 * (size_t)d.npk();
+        T* alt = nullptr;
+        IM3D_TRY(tbuf<T>(ctx, "upk_alt", cnt, &alt));
+        T* cur = U;
+        T* nxt = alt;
+        bool done = false;
+        while (s + 2 <= max_sweeps) {
+            const bool check = s + 2 >= next || s + 2 == max_sweeps;
+            IM3D_TRY(rb_tb_pass<T>(ctx, cur, nxt, B, d, c, check ? (beff2 < 0 ? 2 : 1) : 0));
+            std::swap(cur, nxt);
+            s += 2;
+            if (!check) continue;
+            IM3D_TRY(read_ctrl(ctx));
+            if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
+            const double rr = ctx->ctrl_h->sum[SUM_RES2];
+            const double r = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
+            *rel = r;
+            if (r <= tol) {
+                *conv = true;
+                done = true;
+                break;
+            }
+            next = next_check(s, r, s_prev, r_prev, tol, check_every);
+            if (next > max_sweeps) next = max_sweeps;
+            s_prev = s;
+            r_prev = r;
+        }
+        if (cur != U)
+            IM3D_CUDA(ctx, cudaMemcpyAsync(U, cur, cnt * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+        if (done) {
+            *sweeps = s;
+            return IM3D_OK;
+        }
+    }
     while (s < max_sweeps) {
         IM3D_TRY(rb_sweep(ctx, U, B, d, c, 0, omega));
         ++s;
@@ -1401,6 +1466,8 @@ int im3d_ctx_create(int device, im3d_ctx** out)
     // L2 pinning of the Gauss-Seidel state is opt-in (IM3D_L2_PERSIST=1): on B200 the
     // set-aside speeds the half-sweep up (26.9 -> 22.9 us at 256^3) but slows the
     // streaming kernels of the rest of the iteration more than that
+    const char* tbenv = std::getenv("IM3D_TB");
+    ctx->tb_enabled = tbenv && tbenv[0] == '1';
     const char* pin = std::getenv("IM3D_L2_PERSIST");
     ctx->persist_max = (pin && pin[0] == '1' && prop.persistingL2CacheMaxSize > 0)
                            ? (size_t)prop.persistingL2CacheMaxSize : 0;

@@ -1232,6 +1232,155 @@ __global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
     }
 }
 
+// ---- temporally blocked red-black Gauss-Seidel (two sweeps per pass) ----------
+// One CTA owns a tile of TJ rows x TM packed columns and a chunk of CI planes of i.
+// It streams the planes [c0-4, c1+4) of both colours through a ring of 7 planes in
+// shared memory. When plane q arrives, level L = 1..4 updates colour (L-1)&1 at plane
+// q-L (red, black, red, black: two full sweeps), each level over a region one row and
+// one column smaller than the previous one, so every value a level reads was produced
+// by the level before it. Plane q-4 is then final and is written back (tile interior
+// only); plane q-5 gets the FP64 residual of the result (both colours). The update
+// order inside a colour does not matter, so the result is bit-identical to two calls
+// of rb_sweep.
+template <typename T>
+struct TbRing {
+    static constexpr int LV = 4;      // levels (half-sweeps) per pass
+    static constexpr int H = LV + 1;  // halo: the last level stays valid one cell past the
+                                      // interior, where the residual reads its neighbours
+    static constexpr int NP = 7;      // planes held: q-6 .. q
+};
+
+// The pass is out of place (Uin -> Uout): neighbouring CTAs load overlapping halos of
+// Uin while others write their results, so writing in place would let a CTA read
+// values already advanced by two sweeps.
+template <typename T, int TJ, int TM, int CI>
+__global__ void __launch_bounds__(256) rb_tb2_kernel(const T* __restrict__ Uin, T* __restrict__ Uout,
+                                                     const T* __restrict__ B, Dims d, GsCoef<T> c,
+                                                     double* part,
+                                                     int want_res)  // 0 none, 1 residual, 2 + sum b^2
+{
+    constexpr int H = TbRing<T>::H;
+    constexpr int LV = TbRing<T>::LV;
+    constexpr int NP = TbRing<T>::NP;
+    constexpr int PJ = TJ + 2 * H, PM = TM + 2 * H;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);  // [NP][2][PJ][PM]
+    const int hz = d.hz();
+    const long long plane = (long long)d.ny * hz;
+    const long long npk = plane * d.nx;
+    const int m0 = blockIdx.x * TM, j0 = blockIdx.y * TJ;
+    const int c0 = blockIdx.z * CI;
+    const int c1 = min(c0 + CI, d.nx);
+    const int qa = c0 - H, qb = c1 + H;
+    const int tid = threadIdx.x;
+    const int lo = c.neu ? 0 : 1;
+    auto R = [&](int pl, int col, int jl, int ml) -> T& {
+        return ring[(((pl % NP + NP) % NP) * 2 + col) * PJ * PM + jl * PM + ml];
+    };
+    double racc = 0, bacc = 0;
+    for (int q = qa; q < qb; ++q) {
+        // load plane q (both colours) into the ring
+        if (q >= 0 && q < d.nx && q < qb) {
+            for (int e = tid; e < 2 * PJ * PM; e += blockDim.x) {
+                const int col = e / (PJ * PM);
+                const int r = e - col * PJ * PM;
+                const int jl = r / PM, ml = r - jl * PM;
+                const int j = j0 - H + jl, m = m0 - H + ml;
+                T v = T(0);
+                if (j >= 0 && j < d.ny && m >= 0 && m < hz)
+                    v = Uin[(col ? npk : 0) + (long long)q * plane + (long long)j * hz + m];
+                R(q, col, jl, ml) = v;
+            }
+        }
+        __syncthreads();
+        // levels 1..LV at planes q-1 .. q-LV
+#pragma unroll 1
+        for (int L = 1; L <= LV; ++L) {
+            const int p = q - L;
+            const int color = (L - 1) & 1;
+            if (p >= qa + L && p < qb - L && p >= 0 && p < d.nx) {
+                const int rj = TJ + 2 * (H - L), rm = TM + 2 * (H - L);
+                for (int e = tid; e < rj * rm; e += blockDim.x) {
+                    const int jl = L + e / rm, ml = L + e % rm;
+                    const int j = j0 - H + jl, m = m0 - H + ml;
+                    if (j < 0 || j >= d.ny || m < 0 || m >= hz) continue;
+                    const int i = p;
+                    const int par = (i + j + color) & 1;
+                    const int k = 2 * m + par;
+                    if (k >= d.nz) continue;
+                    if (i < lo || j < lo || k < lo || i >= d.nx - lo || j >= d.ny - lo || k >= d.nz - lo)
+                        continue;
+                    const int oc = 1 - color;
+                    const T b = B[(color ? npk : 0) + (long long)p * plane + (long long)j * hz + m];
+                    const bool interior = i >= 1 && i <= d.nx - 2 && j >= 1 && j <= d.ny - 2 &&
+                                          k >= 1 && k <= d.nz - 2;
+                    T v;
+                    if (interior) {
+                        const T sx = R(p - 1, oc, jl, ml) + R(p + 1, oc, jl, ml);
+                        const T sy = R(p, oc, jl - 1, ml) + R(p, oc, jl + 1, ml);
+                        const T sz = R(p, oc, jl, ml) + (par ? R(p, oc, jl, ml + 1) : R(p, oc, jl, ml - 1));
+                        if (std::is_same<T, double>::value) {
+                            double acc = sx / (c.hx * c.hx) + sy / (c.hy * c.hy) + sz / (c.hz * c.hz) + b;
+                            v = T(acc * (double)c.htilde[7]);
+                        } else {
+                            v = fma(sx, c.ihx2, fma(sy, c.ihy2, fma(sz, c.ihz2, b))) * c.htilde[7];
+                        }
+                    } else {
+                        // Neumann boundary point: only in-domain neighbours are read
+                        auto rd = [&](int oi, int oj, int ok) -> T {
+                            const int mm = (k + ok) >> 1;
+                            return R(p + oi, oc, jl + oj, mm - (m0 - H));
+                        };
+                        v = gs_value<T>(c, d, i, j, k, b, T(0), false, rd);
+                    }
+                    R(p, color, jl, ml) = v;
+                }
+            }
+            __syncthreads();
+        }
+        // write back plane q-LV (final after level LV)
+        const int pw = q - LV;
+        if (pw >= c0 && pw < c1) {
+            for (int e = tid; e < 2 * TJ * TM; e += blockDim.x) {
+                const int col = e / (TJ * TM);
+                const int r = e - col * TJ * TM;
+                const int jl = H + r / TM, ml = H + r % TM;
+                const int j = j0 - H + jl, m = m0 - H + ml;
+                if (j < d.ny && m < hz)
+                    Uout[(col ? npk : 0) + (long long)pw * plane + (long long)j * hz + m] = R(pw, col, jl, ml);
+            }
+        }
+        // FP64 residual of the final state at plane q-LV-1 (planes q-LV-2 .. q-LV final)
+        const int pr = q - LV - 1;
+        if (want_res && pr >= c0 && pr < c1) {
+            for (int e = tid; e < 2 * TJ * TM; e += blockDim.x) {
+                const int col = e / (TJ * TM);
+                const int r = e - col * TJ * TM;
+                const int jl = H + r / TM, ml = H + r % TM;
+                const int j = j0 - H + jl, m = m0 - H + ml;
+                if (j >= d.ny || m >= hz) continue;
+                const int i = pr;
+                const int k = 2 * m + ((i + j + col) & 1);
+                if (k >= d.nz) continue;
+                if (i < lo || j < lo || k < lo || i >= d.nx - lo || j >= d.ny - lo || k >= d.nz - lo)
+                    continue;
+                const int oc = 1 - col;
+                auto rd = [&](int oi, int oj, int ok) -> double {
+                    const int mm = (k + ok) >> 1;
+                    return (double)R(pr + oi, oc, jl + oj, mm - (m0 - H));
+                };
+                const double bv = (double)B[(col ? npk : 0) + (long long)pr * plane + (long long)j * hz + m];
+                const double rr = gs_residual_fp64<T>(c, d, i, j, k, bv, (double)R(pr, col, jl, ml), rd);
+                racc += rr * rr;
+                bacc += bv * bv;
+            }
+        }
+        __syncthreads();
+    }
+    if (want_res == 2) block_sum2_store(racc, bacc, part);
+    else if (want_res) block_sum_store(racc, part);
+}
+
 // ---- vectorised natural-layout kernels (nz a multiple of W = 16/sizeof(T)) ----
 // Thread per group of W consecutive k of row j, marching over NI planes of i.
 

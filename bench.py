@@ -55,6 +55,16 @@ ALGO_BYTES_PER_VOXEL = {
     "conv_k_rhs": 28.0,       # pair 8, u0 4, div(d-b) 4, phi 4 read; packed b_eff 4, u 4 write
     "post_solve": 52.0,       # u 4, phiold 4, b 12, g 4 read; phi 4, b 12, d-b 12 write
     "div": 16.0,              # d-b read 12, div write 4
+    "clamp_tol": 12.0,        # packed u read 4, phiold read 4, phi write 4
+    "bregman": 44.0,          # phi 4, b 12, g 4 read; b 12, d-b 12 write
+    "rb_tb2": 12.0,           # one pass = two sweeps: u read 4, b_eff read 4, u write 4
+}
+
+WORKLOADS = {
+    # the headline
+    "c2": dict(shape=(256, 256, 256), maxiter=100, sigma=3.0),
+    # CT-shaped single volume
+    "c3": dict(shape=(512, 512, 320), maxiter=200, sigma=4.0),
 }
 
 
@@ -145,9 +155,12 @@ def run_gpu(args):
                                 device_id=torch.device("cuda", local))
     pkg = importlib.import_module("3dimagetoolkit_b200")
 
-    shape = SHAPE if not args.size else (args.size,) * 3
+    wl = WORKLOADS[args.workload]
+    shape = wl["shape"] if not args.size else (args.size,) * 3
     n = shape[0] * shape[1] * shape[2]
-    if args.size:
+    if args.workload == "c3" and not args.size:
+        u0_np, phi0_np = pkg.synth.config_volume("c3", seed=args.seed + rank, dtype=np.float32)
+    elif args.size:
         u0_np = pkg.synth.ellipsoids(shape, args.seed + rank, n=8, semi_axes=(10, 40),
                                      fg_range=(0.6, 0.9), bias=(0.7, 1.3), noise=0.05,
                                      dtype=np.float32)
@@ -168,6 +181,8 @@ def run_gpu(args):
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     kw = dict(PARAMS)
+    kw["maxiter"] = wl["maxiter"]
+    kw["sigma"] = wl["sigma"]
     if args.maxiter:
         kw["maxiter"] = args.maxiter
     params = pkg.default_params(**kw)
@@ -273,16 +288,19 @@ def run_gpu(args):
         per_step_ms = dt_ms / args.steps
         roofline["step_algo_gb"] = algo_step / 1e9
         roofline["step_frac"] = (algo_step / (per_step_ms * 1e-3) / 1e9) / peak
-        stages = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in
-                  sorted(prof.items(), key=lambda kv: -kv[1][0])}
+        stages = {k: {"ms": round(v[0], 3), "launches": v[1],
+                      "algo_gbs": (round(ALGO_BYTES_PER_VOXEL[k] * n * v[1] / (v[0] * 1e-3) / 1e9, 1)
+                                   if k in ALGO_BYTES_PER_VOXEL and v[0] > 0 else None)}
+                  for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded ellipsoid volumes, one per rank)",
-            "config": {"workload": "rsfe-sb 256^3 fp32, 100 outer iterations, RB-GS to rel. "
-                                   "residual 1e-6", "shape": list(shape), "outer_iterations": MAXITER,
-                       "sigma": 3.0, "volumes_per_rank": 1, "parallelism": f"replicas x{ws} (one volume per GPU)",
+            "config": {"workload": (f"rsfe-sb {shape[0]}x{shape[1]}x{shape[2]} fp32, "
+                                    f"{kw['maxiter']} outer iterations, RB-GS to rel. residual 1e-6"),
+                       "shape": list(shape), "outer_iterations": kw["maxiter"],
+                       "sigma": kw["sigma"], "volumes_per_rank": 1, "parallelism": f"replicas x{ws} (one volume per GPU)",
                        "l2": "working set ~2 GB > 126 MB L2, no flush needed",
                        "gs_sweeps_per_step": sweeps / max(args.steps, 1)},
             "e2e": {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 4,
@@ -290,7 +308,9 @@ def run_gpu(args):
             "roofline": roofline, "stages_ms_per_step": stages, "gpu_launches": launches,
             "clocks": clocks,
         }
-        if ws == 1 and not args.no_cpu:
+        if args.workload != "c2":
+            result["metric"] = METRIC.replace("@256^3", "@%dx%dx%d" % tuple(shape))
+        if ws == 1 and not args.no_cpu and args.workload == "c2":
             result["cpu_baseline"] = cpu_baseline(args)
     ctx.close()
     if ws > 1:
@@ -321,7 +341,8 @@ def run_batch(args):
                                 device_id=torch.device("cuda", local))
     pkg = importlib.import_module("3dimagetoolkit_b200")
     shapes = pkg.synth.batch_shapes(48, seed=args.seed)
-    mine = [q for q in range(len(shapes)) if q % ws == rank]  # volumes shard across ranks
+    shard = importlib.import_module("3dimagetoolkit_b200.shard")
+    mine = shard.volume_shard(len(shapes), rank, ws)  # volumes shard across ranks
     dev = torch.device("cuda", local)
     vols, inits, outs = [], [], []
     for q in mine:
@@ -350,12 +371,7 @@ def run_batch(args):
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     launches = ctx.launches - launches0
-    if ws > 1:
-        t = torch.tensor([dt, vox_iters], dtype=torch.float64, device=dev)
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        dt, vox_iters = float(mx[0]), float(t[1])
+    vox_iters, dt = shard.job_throughput(vox_iters, dt)
     ctx.close()
     if rank == 0:
         line = {
@@ -444,8 +460,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="c2", choices=["c2", "batch"],
-                    help="c2: one 256^3 volume per step (default); batch: 48 uneven volumes")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batch"],
+                    help="c2: one 256^3 volume per step (default); c3: 512x512x320 CT-like "
+                         "volume, sigma 4, 200 iterations; batch: 48 uneven volumes")
     ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent streams")
     ap.add_argument("--size", type=int, default=0,
                     help="profiling only: cube side of a smaller/larger case (default 256)")
