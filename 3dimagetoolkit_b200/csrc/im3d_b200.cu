@@ -61,6 +61,8 @@ struct im3d_ctx {
     bool persist_set = false;
     // temporally blocked sweep pairs for FP32 solves (opt-in: IM3D_TB=1)
     bool tb_enabled = false;
+    int pair_resident[2] = {0, 0};  // resident rb_pair_kernel CTAs (24- and 22-row tiles)
+    int num_sms = 148;
 };
 
 namespace {
@@ -652,27 +654,80 @@ void l2_unpin(im3d_ctx* ctx)
     if (cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
 }
 
-// Two red-black sweeps in one temporally blocked pass (rb_tb2_kernel), optionally
-// with the FP64 residual of the result (want_res 1) and sum b_eff^2 (want_res 2)
-// folded into ctrl->sum[SUM_RES2 ..].
-constexpr int kTbJ = 16, kTbM = 32, kTbI = 32;
-
-template <typename T>
-int rb_tb_pass(im3d_ctx* ctx, const T* Uin, T* Uout, const T* B, const Dims& d, const GsCoef<T>& c,
-               int want_res)
+// Two red-black sweeps in one temporally blocked pass (rb_pair_kernel, FP32).
+// Tiles of 8 float4 columns (32 packed cells) by 24 or 22 rows; the tile height and
+// the chunk of planes per CTA are chosen to minimise the work of the busiest SM,
+// ceil(ctas / resident) * (chunk + 8) * threads per CTA, so that the CTAs fill whole
+// waves of the GPU.
+template <int TJ>
+int rb_pair_plan(im3d_ctx* ctx, const Dims& d, int slot, long long* cost, int* ci_out)
 {
-    constexpr int H = TbRing<T>::H, NP = TbRing<T>::NP;
-    const size_t smem = (size_t)NP * 2 * (kTbJ + 2 * H) * (kTbM + 2 * H) * sizeof(T);
-    auto kern = rb_tb2_kernel<T, kTbJ, kTbM, kTbI>;
-    IM3D_TRY(set_smem(ctx, kern, smem));
-    const dim3 grid((d.hz() + kTbM - 1) / kTbM, (d.ny + kTbJ - 1) / kTbJ, (d.nx + kTbI - 1) / kTbI);
-    double* part = nullptr;
-    if (want_res) IM3D_TRY(part_buf(ctx, grid, want_res == 2 ? 2 : 1, &part));
-    const int pf = prof_begin(ctx, "rb_tb2");
-    kern<<<grid, 256, smem, ctx->stream>>>(Uin, Uout, B, d, c, part, want_res);
+    using G = TbGeom<TJ, 8>;
+    auto kern = rb_pair_kernel<TJ, 8>;
+    if (ctx->pair_resident[slot] <= 0) {
+        IM3D_TRY(set_smem(ctx, kern, G::SMEM));
+        int per_sm = 0;
+        IM3D_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::NT, G::SMEM));
+        if (per_sm < 1) return fail(ctx, IM3D_ERR_CUDA, "rb_pair_kernel does not fit on an SM");
+        ctx->pair_resident[slot] = per_sm * ctx->num_sms;
+    }
+    const long long tiles = (long long)((d.hz() + 31) / 32) * ((d.ny + TJ - 1) / TJ);
+    *cost = -1;
+    for (int ci = 8; ci <= d.nx; ++ci) {
+        const long long chunks = (d.nx + ci - 1) / ci;
+        const long long waves = (tiles * chunks + ctx->pair_resident[slot] - 1) / ctx->pair_resident[slot];
+        const long long cst = waves * (ci + 8) * G::NT;
+        if (*cost < 0 || cst < *cost) {
+            *cost = cst;
+            *ci_out = ci;
+        }
+    }
+    return IM3D_OK;
+}
+
+template <int TJ>
+int rb_pair_launch(im3d_ctx* ctx, const float* Uin, float* Uout, const float* B, const Dims& d,
+                   const GsCoef<float>& c, int ci)
+{
+    using G = TbGeom<TJ, 8>;
+    const long long tiles = (long long)((d.hz() + 31) / 32) * ((d.ny + TJ - 1) / TJ);
+    const dim3 grid((unsigned)tiles, (unsigned)((d.nx + ci - 1) / ci));
+    const int pf = prof_begin(ctx, "rb_pair");
+    rb_pair_kernel<TJ, 8><<<grid, G::NT, G::SMEM, ctx->stream>>>(Uin, Uout, B, d, c, ci);
     prof_end(ctx, pf);
-    IM3D_TRY(check_launch(ctx, "rb_tb2"));
-    if (want_res) IM3D_TRY(finalize(ctx, part, grid, want_res == 2 ? 2 : 1, SUM_RES2));
+    return check_launch(ctx, "rb_pair");
+}
+
+int rb_pair_pass(im3d_ctx* ctx, const float* Uin, float* Uout, const float* B, const Dims& d,
+                 const GsCoef<float>& c)
+{
+    long long c24 = 0, c22 = 0;
+    int ci24 = 0, ci22 = 0;
+    IM3D_TRY(rb_pair_plan<24>(ctx, d, 0, &c24, &ci24));
+    IM3D_TRY(rb_pair_plan<22>(ctx, d, 1, &c22, &ci22));
+    if (c22 < c24) return rb_pair_launch<22>(ctx, Uin, Uout, B, d, c, ci22);
+    return rb_pair_launch<24>(ctx, Uin, Uout, B, d, c, ci24);
+}
+
+// FP64 residual of the packed state, and sum b_eff^2 on the first call (*beff2 < 0);
+// returns the relative residual in *rel.
+template <typename T>
+int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<T>& c,
+             double* beff2, double* rel)
+{
+    const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2);
+    const int nvals = *beff2 < 0 ? 2 : 1;
+    double* part = nullptr;
+    IM3D_TRY(part_buf(ctx, grid, nvals, &part));
+    const int pf = prof_begin(ctx, "rb_residual");
+    rb_residual_vec_kernel<T, kNV><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
+    prof_end(ctx, pf);
+    IM3D_TRY(check_launch(ctx, "rb_residual"));
+    IM3D_TRY(finalize(ctx, part, grid, nvals, SUM_RES2));
+    IM3D_TRY(read_ctrl(ctx));
+    if (*beff2 < 0) *beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
+    const double rr = ctx->ctrl_h->sum[SUM_RES2];
+    *rel = *beff2 > 0 ? std::sqrt(rr) / std::sqrt(*beff2) : std::sqrt(rr);
     return IM3D_OK;
 }
 
@@ -695,63 +750,49 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
         im3d_ctx* c;
         ~Unpin() { l2_unpin(c); }
     } unpin{ctx};
-    // FP32 with omega == 1: sweeps go in temporally blocked pairs, and the residual
-    // of a pair comes out of the same pass; checks land on pair boundaries
-    const bool tb = sizeof(T) == 4 && omega == 1.0 && ctx->tb_enabled && max_sweeps >= 2;
-    if (tb) {
-        // passes alternate between U and a second packed buffer
-        const size_t cnt = 2 * (size_t)d.npk();
-        T* alt = nullptr;
-        IM3D_TRY(tbuf<T>(ctx, "upk_alt", cnt, &alt));
-        T* cur = U;
-        T* nxt = alt;
-        bool done = false;
-        while (s + 2 <= max_sweeps) {
-            const bool check = s + 2 >= next || s + 2 == max_sweeps;
-            IM3D_TRY(rb_tb_pass<T>(ctx, cur, nxt, B, d, c, check ? (beff2 < 0 ? 2 : 1) : 0));
-            std::swap(cur, nxt);
-            s += 2;
-            if (!check) continue;
-            IM3D_TRY(read_ctrl(ctx));
-            if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
-            const double rr = ctx->ctrl_h->sum[SUM_RES2];
-            const double r = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
-            *rel = r;
-            if (r <= tol) {
-                *conv = true;
-                done = true;
-                break;
+    // FP32 with omega == 1: sweeps go in temporally blocked pairs; checks land on pair
+    // boundaries (at most one sweep past the scheduled one)
+    if constexpr (std::is_same<T, float>::value) {
+        if (omega == 1.0 && ctx->tb_enabled && max_sweeps >= 2) {
+            const size_t cnt = 2 * (size_t)d.npk();
+            T* alt = nullptr;
+            IM3D_TRY(tbuf<T>(ctx, "upk_alt", cnt, &alt));
+            T* cur = U;
+            T* nxt = alt;
+            bool done = false;
+            while (s + 2 <= max_sweeps) {
+                IM3D_TRY(rb_pair_pass(ctx, cur, nxt, B, d, c));
+                std::swap(cur, nxt);
+                s += 2;
+                if (s < next && s != max_sweeps) continue;
+                double r = 0;
+                IM3D_TRY(rb_check<T>(ctx, cur, B, d, c, &beff2, &r));
+                *rel = r;
+                if (r <= tol) {
+                    *conv = true;
+                    done = true;
+                    break;
+                }
+                next = next_check(s, r, s_prev, r_prev, tol, check_every);
+                if (next > max_sweeps) next = max_sweeps;
+                s_prev = s;
+                r_prev = r;
             }
-            next = next_check(s, r, s_prev, r_prev, tol, check_every);
-            if (next > max_sweeps) next = max_sweeps;
-            s_prev = s;
-            r_prev = r;
-        }
-        if (cur != U)
-            IM3D_CUDA(ctx, cudaMemcpyAsync(U, cur, cnt * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
-        if (done) {
-            *sweeps = s;
-            return IM3D_OK;
+            if (cur != U)
+                IM3D_CUDA(ctx, cudaMemcpyAsync(U, cur, cnt * sizeof(T), cudaMemcpyDeviceToDevice,
+                                               ctx->stream));
+            if (done || s == max_sweeps) {
+                *sweeps = s;
+                return IM3D_OK;
+            }
         }
     }
     while (s < max_sweeps) {
         IM3D_TRY(rb_sweep(ctx, U, B, d, c, 0, omega));
         ++s;
         if (s >= next || s == max_sweeps) {
-            const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2);
-            const int nvals = beff2 < 0 ? 2 : 1;
-            double* part = nullptr;
-            IM3D_TRY(part_buf(ctx, grid, nvals, &part));
-            const int pf = prof_begin(ctx, "rb_residual");
-            rb_residual_vec_kernel<T, kNV><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part,
-                                                                            nvals == 2 ? 1 : 0);
-            prof_end(ctx, pf);
-            IM3D_TRY(check_launch(ctx, "rb_residual"));
-            IM3D_TRY(finalize(ctx, part, grid, nvals, SUM_RES2));
-            IM3D_TRY(read_ctrl(ctx));
-            if (beff2 < 0) beff2 = ctx->ctrl_h->sum[SUM_BEFF2];
-            const double rr = ctx->ctrl_h->sum[SUM_RES2];
-            const double r = beff2 > 0 ? std::sqrt(rr) / std::sqrt(beff2) : std::sqrt(rr);
+            double r = 0;
+            IM3D_TRY(rb_check<T>(ctx, U, B, d, c, &beff2, &r));
             *rel = r;
             if (r <= tol) {
                 *conv = true;
@@ -1472,6 +1513,7 @@ int im3d_ctx_create(int device, im3d_ctx** out)
     ctx->persist_max = (pin && pin[0] == '1' && prop.persistingL2CacheMaxSize > 0)
                            ? (size_t)prop.persistingL2CacheMaxSize : 0;
     ctx->window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
+    ctx->num_sms = prop.multiProcessorCount;
     *out = ctx;
     return IM3D_OK;
 }

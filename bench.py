@@ -57,7 +57,7 @@ ALGO_BYTES_PER_VOXEL = {
     "div": 16.0,              # d-b read 12, div write 4
     "clamp_tol": 12.0,        # packed u read 4, phiold read 4, phi write 4
     "bregman": 44.0,          # phi 4, b 12, g 4 read; b 12, d-b 12 write
-    "rb_tb2": 12.0,           # one pass = two sweeps: u read 4, b_eff read 4, u write 4
+    "rb_pair": 12.0,           # one pass = two sweeps: u read 4, b_eff read 4, u write 4
 }
 
 WORKLOADS = {
