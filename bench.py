@@ -301,7 +301,8 @@ def run_gpu(args):
                                     f"{kw['maxiter']} outer iterations, RB-GS to rel. residual 1e-6"),
                        "shape": list(shape), "outer_iterations": kw["maxiter"],
                        "sigma": kw["sigma"], "volumes_per_rank": 1, "parallelism": f"replicas x{ws} (one volume per GPU)",
-                       "l2": "working set ~2 GB > 126 MB L2, no flush needed",
+                       "l2": (f"every field {n * 4 / 2**20:.0f} MiB and each pass streams "
+                              "several of them: inputs larger than the 126 MB L2, no flush"),
                        "gs_sweeps_per_step": sweeps / max(args.steps, 1)},
             "e2e": {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 4,
                     "d2h_bytes_per_step": n * 4, "ms_per_step": e_ms / args.steps},
