@@ -412,6 +412,16 @@ def _ref_iteration_seconds(shape, maxiter, seed):
     return [float(x) for x in steps]
 
 
+def _cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(args):
     cores = os.cpu_count()
     t0 = time.time()
@@ -421,6 +431,7 @@ def cpu_baseline(args):
     log(f"cpu baseline: {len(secs)} timed iteration(s), {per_it:.2f} s each, "
         f"{time.time() - t0:.1f} s total")
     return {"value": n / per_it / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+            "cpu_model": _cpu_model(),
             "sample": "reference C++ (oracle/_ref: the reference headers, FFTW replaced by an "
                       "in-tree FP64 FFT, VTK/GetPot by headless shims), T=double, 256^3, "
                       "wall time of outer iteration 2 of 2 (setup and iteration 1 excluded), "
@@ -446,6 +457,7 @@ def run_reference(args):
         "config": {"workload": "rsfe-sb 256^3, one outer iteration per step, Poisson step solved "
                                "to rel. residual 1e-6 (red-black plug-in)", "shape": list(SHAPE)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "cpu_model": _cpu_model(),
                          "sample": f"{len(timed)} outer iterations of the 256^3 workload after "
                                    f"{args.warmup} warm-up iterations and the set-up"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
