@@ -54,6 +54,10 @@ class RsfeParams(C.Structure):
         ("maxiter", C.c_int32), ("ls_steps", C.c_int32), ("bc", C.c_int32),
         ("gaussian_pixel_approach", C.c_int32), ("init_variables", C.c_int32),
         ("sweep", C.c_int32), ("gs_max_sweeps", C.c_int32), ("gs_check_every", C.c_int32),
+        ("cc_init_pixel_x", C.c_double), ("cc_init_pixel_y", C.c_double),
+        ("cc_init_pixel_z", C.c_double), ("alpha", C.c_double),
+        ("auto_extract_conn_comp", C.c_int32), ("auto_extract_conn_comp_freq", C.c_int32),
+        ("cc_binary_output", C.c_int32), ("cc_init_variables", C.c_int32),
     ]
 
     def as_dict(self):
@@ -237,6 +241,21 @@ class Context:
         fn = getattr(lib(), "im3d_div_" + _suffix(dt))
         self._check(fn(self._h, pv, po, *map(C.c_int, out.shape), *map(C.c_double, h)))
         return out
+
+    def connected_component(self, img, ijk=(0, 0, 0), init=None, threshold=0.5,
+                            full_connected=False, binary_output=True, out=None,
+                            return_passes=False):
+        """image3d<T>::connected_component: seeded by cell ``ijk`` (init None) or by the
+        cells where ``init`` != 0; returns the result (and the growth passes)."""
+        pi, dtp = _ptr(img)
+        pinit, _ = _ptr(init)
+        res = _empty_like(img) if out is None else out
+        passes = C.c_int(0)
+        fn = getattr(lib(), "im3d_connected_component_" + _suffix(dtp))
+        self._check(fn(self._h, pi, _ptr(res)[0], *map(C.c_int, img.shape), pinit,
+                       *map(C.c_int, ijk), C.c_double(threshold), C.c_int(int(full_connected)),
+                       C.c_int(int(binary_output)), C.byref(passes)))
+        return (res, int(passes.value)) if return_passes else res
 
     def poisson_sweeps(self, res, b, dt=1.0, bc=0.0, bc_type=BC_DIR, order=SWEEP_LEXICOGRAPHIC,
                        sweeps=1, h=(1.0, 1.0, 1.0)):

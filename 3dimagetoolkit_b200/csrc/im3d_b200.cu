@@ -808,6 +808,161 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
     return IM3D_OK;
 }
 
+// Exact minimum and maximum of a device volume (FP64 order keys of the values).
+double order_key_to_double(unsigned long long k)
+{
+    unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    return v;
+}
+
+template <typename T>
+int minmax(im3d_ctx* ctx, const T* p, long long n, T* mn, T* mx)
+{
+    IM3D_CUDA(ctx, cudaMemsetAsync(ctx->ctrl_d->umax, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    minmax_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(p, n, ctx->ctrl_d->umax);
+    IM3D_TRY(check_launch(ctx, "minmax"));
+    IM3D_TRY(read_ctrl(ctx));
+    *mx = (T)order_key_to_double(ctx->ctrl_h->umax[0]);
+    *mn = (T)(-order_key_to_double(ctx->ctrl_h->umax[1]));
+    return IM3D_OK;
+}
+
+// image3d<T>::connected_component (image3d_imp.hxx:1694-2120) on device buffers; res
+// may be img (the result is written element by element after the last read).
+template <typename T>
+int cc_run(im3d_ctx* ctx, const T* img, T* res, const Dims& d, const T* init, int i, int j, int k,
+           double threshold, int full, int binary, int* passes)
+{
+    const long long n = d.n();
+    T mn, mx;
+    IM3D_TRY(minmax<T>(ctx, img, n, &mn, &mx));
+    if (threshold > 1 || threshold < 0) {
+        ctx->err = "WARNING::im_to_black_and_white: threshold must be between 0 and 1, "
+                   "otherwise default value 0.5 is applied";
+        threshold = 0.5;
+    }
+    // pivot (min + (max - min) * threshold), the difference in T (image3d_imp.hxx:1603)
+    const T span = mx - mn;
+    const T pivot = (T)((double)mn + (double)span * threshold);
+    int negative = 0;
+    long long seed = -1;
+    if (!init) {
+        // the seed moved off the faces (:1700-1736)
+        unsigned I = (unsigned)i, J = (unsigned)j, K = (unsigned)k;
+        if (I == 0) ++I;
+        if (J == 0) ++J;
+        if (I >= (unsigned)d.nx - 1) I = d.nx - 2;
+        if (J >= (unsigned)d.ny - 1) J = d.ny - 2;
+        if (d.nz == 1) {
+            K = 0;
+        } else {
+            if (K == 0) ++K;
+            if (K >= (unsigned)d.nz - 1) K = d.nz - 2;
+        }
+        seed = d.idx((int)I, (int)J, (int)K);
+        T v;
+        IM3D_CUDA(ctx, cudaMemcpyAsync(&v, img + seed, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+        IM3D_TRY(sync(ctx));
+        negative = v < pivot;  // a dark seed: the component of the negative image (:1740-1745)
+    }
+    unsigned char* m0 = nullptr;
+    unsigned char* m1 = nullptr;
+    IM3D_TRY(tbuf<unsigned char>(ctx, "cc_mask0", (size_t)n, &m0));
+    IM3D_TRY(tbuf<unsigned char>(ctx, "cc_mask1", (size_t)n, &m1));
+    cc_init_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(img, init, m0, n, pivot, negative, seed);
+    IM3D_TRY(check_launch(ctx, "cc_init"));
+    const dim3 grid((d.nz + kCcK - 1) / kCcK, (d.ny + kCcJ - 1) / kCcJ, (d.nx + kCcI - 1) / kCcI);
+    const dim3 blk(kCcK, kCcJ);
+    unsigned long long* flag = ctx->ctrl_d->umax + 2;
+    long long np = 0;
+    for (;;) {
+        IM3D_CUDA(ctx, cudaMemsetAsync(flag, 0, sizeof(unsigned long long), ctx->stream));
+        for (int r = 0; r < 4; ++r) {
+            const int pf = prof_begin(ctx, "cc_grow");
+            if (full) cc_grow_kernel<true><<<grid, blk, 0, ctx->stream>>>(m0, m1, d, flag);
+            else cc_grow_kernel<false><<<grid, blk, 0, ctx->stream>>>(m0, m1, d, flag);
+            prof_end(ctx, pf);
+            IM3D_TRY(check_launch(ctx, "cc_grow"));
+            std::swap(m0, m1);
+            ++np;
+        }
+        IM3D_TRY(read_ctrl(ctx));
+        if (ctx->ctrl_h->umax[2] == 0) break;
+        // every pass that does not end the loop adds a cell
+        if (np > n + 8) return fail(ctx, IM3D_ERR_CUDA, "connected_component: no fixed point");
+    }
+    cc_output_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(m0, img, res, n, binary, mn, pivot);
+    IM3D_TRY(check_launch(ctx, "cc_output"));
+    if (passes) *passes = (int)(np < 0x7fffffff ? np : 0x7fffffff);
+    return IM3D_OK;
+}
+
+template <typename T>
+int connected_component_op(im3d_ctx* ctx, const T* img_user, T* res_user, int nx, int ny, int nz,
+                           const T* init_user, int i, int j, int k, double threshold, int full,
+                           int binary, int* passes)
+{
+    if (!img_user || !res_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
+    if (nx < 2 || ny < 2 || nz < 1)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "connected_component needs nx, ny >= 2 and nz >= 1");
+    if ((long long)nx * ny > 0x7fffffffLL || nx > 262000 || ny > 524000)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "volume too large for the launch geometry");
+    ctx->err.clear();
+    const Dims d{nx, ny, nz};
+    const T* img = nullptr;
+    const T* init = nullptr;
+    T* res = nullptr;
+    IM3D_TRY(dev_in<T>(ctx, img_user, d.n(), "in_a", &img));
+    if (init_user) IM3D_TRY(dev_in<T>(ctx, init_user, d.n(), "in_b", &init));
+    IM3D_TRY(dev_out<T>(ctx, res_user, d.n(), "out_a", &res));
+    IM3D_TRY(cc_run<T>(ctx, img, res, d, init, i, j, k, threshold, full, binary, passes));
+    IM3D_TRY(out_finish<T>(ctx, res_user, res, d.n()));
+    return sync(ctx);
+}
+
+// extract_connected_component, automatic case (rsfe_splitbregman_imp.hxx:448-536), on
+// the clamped level set: *replaced = true when phi became its (rescaled) component.
+template <typename T>
+int extract_cc(im3d_ctx* ctx, T* phi, const Dims& d, double hx, double hy, double hz,
+               const im3d_rsfe_params* p, bool* replaced)
+{
+    *replaced = false;
+    const int i = (int)std::floor(p->cc_init_pixel_x / hx);
+    const int j = (int)std::floor(p->cc_init_pixel_y / hy);
+    const int k = (int)std::floor(p->cc_init_pixel_z / hz);
+    if (i < 0 || j < 0 || (d.nz != 1 && k < 0)) return IM3D_OK;
+    const unsigned I = (unsigned)i, J = (unsigned)j, K = (unsigned)k;
+    if (I > (unsigned)d.nx - 1 || J > (unsigned)d.ny - 1 || (d.nz != 1 && K > (unsigned)d.nz - 1))
+        return IM3D_OK;
+    // white at the seed after im_to_black_and_white(phi, (alpha - a0) / (b0 - a0)), in T
+    const T alpha = (T)p->alpha, a0 = (T)p->a0, b0 = (T)p->b0;
+    double thr = (double)((alpha - a0) / (b0 - a0));
+    if (thr > 1 || thr < 0) thr = 0.5;
+    T mn, mx;
+    IM3D_TRY(minmax<T>(ctx, phi, d.n(), &mn, &mx));
+    const T span = mx - mn;
+    const T pivot = (T)((double)mn + (double)span * thr);
+    T v;
+    IM3D_CUDA(ctx, cudaMemcpyAsync(&v, phi + d.idx((int)I, (int)J, (int)K), sizeof(T),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    IM3D_TRY(sync(ctx));
+    if (v < pivot) return IM3D_OK;
+    // phi = connected_component(phi, I, J, K, 0.5, face connectivity, cc_binary_output)
+    IM3D_TRY(cc_run<T>(ctx, phi, phi, d, nullptr, (int)I, (int)J, (int)K, 0.5, 0,
+                       p->cc_binary_output, nullptr));
+    // change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636)
+    T cmn, cmx;
+    IM3D_TRY(minmax<T>(ctx, phi, d.n(), &cmn, &cmx));
+    const T shifted_max = cmx - cmn;
+    const T sc = shifted_max / (b0 - a0);
+    affine_kernel<T><<<flat_grid(d.n()), 256, 0, ctx->stream>>>(phi, d.n(), cmn, sc, a0);
+    IM3D_TRY(check_launch(ctx, "affine"));
+    *replaced = true;
+    return IM3D_OK;
+}
+
 // --------------------------------------------------------------- the loop
 template <typename T>
 struct Outs {
@@ -901,17 +1056,8 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     }
     {
         IM3D_TRY(zero_ctrl(ctx));
-        minmax_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(phiA, n, ctx->ctrl_d->umax);
-        IM3D_TRY(check_launch(ctx, "minmax"));
-        IM3D_TRY(read_ctrl(ctx));
-        auto key_to_double = [](unsigned long long k) {
-            unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
-            double v;
-            std::memcpy(&v, &b, sizeof v);
-            return v;
-        };
-        const T mx = (T)key_to_double(ctx->ctrl_h->umax[0]);
-        const T mn = (T)(-key_to_double(ctx->ctrl_h->umax[1]));
+        T mn, mx;
+        IM3D_TRY(minmax<T>(ctx, phiA, n, &mn, &mx));
         const T shifted_max = mx - mn;
         const T s = shifted_max / (T)(b0 - a0);
         affine_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(phiA, n, mn, s, a0);
@@ -1027,6 +1173,16 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
 
         // clamp, tolerance, Bregman update, div(d - b)
         T* phi_new = lex ? other : phi;  // lex: `other` holds phiold and receives the clamp
+        // automatic connected-component extraction at this iteration (:1809): phiold is
+        // kept for the tolerance, which the reference takes after the extraction
+        const bool cc_now = p->auto_extract_conn_comp && p->auto_extract_conn_comp_freq != 0 &&
+                            t % p->auto_extract_conn_comp_freq == 0;
+        T* cc_old = nullptr;
+        if (cc_now) {
+            IM3D_TRY(tbuf<T>(ctx, "cc_phiold", (size_t)n, &cc_old));
+            IM3D_CUDA(ctx, cudaMemcpyAsync(cc_old, phi_new, n * sizeof(T), cudaMemcpyDeviceToDevice,
+                                           ctx->stream));
+        }
         // vector path: rows 16-byte aligned (nz multiple of the width) and an aligned u_out
         const bool vec = d.nz % V16<T>::W == 0 && ((uintptr_t)u_d % 16) == 0;
         {
@@ -1050,6 +1206,19 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             prof_end(ctx, pf);
             IM3D_TRY(check_launch(ctx, "clamp_tol"));
             IM3D_TRY(finalize(ctx, part, grid, 2, SUM_DPHI2));
+        }
+        if (cc_now) {
+            bool replaced = false;
+            IM3D_TRY(extract_cc<T>(ctx, phi_new, d, hx, hy, hz, p, &replaced));
+            if (replaced) {
+                if (p->cc_init_variables) init_variables = 1;
+                const dim3 grid(flat_grid(n));
+                double* part = nullptr;
+                IM3D_TRY(part_buf(ctx, grid, 2, &part));
+                diff_sums_kernel<T><<<grid, 256, 0, ctx->stream>>>(phi_new, cc_old, n, part);
+                IM3D_TRY(check_launch(ctx, "diff_sums"));
+                IM3D_TRY(finalize(ctx, part, grid, 2, SUM_DPHI2));
+            }
         }
         if (init_variables) {
             IM3D_CUDA(ctx, cudaMemsetAsync(divdb, 0, n * sizeof(T), ctx->stream));
@@ -1617,6 +1786,15 @@ void im3d_rsfe_params_default(im3d_rsfe_params* p)
     p->omega = 1.0;
     p->gs_max_sweeps = 1000;
     p->gs_check_every = 0;
+    // connected-component extraction (rsfe_splitbregman_imp.hxx:32-33, 40)
+    p->cc_init_pixel_x = -1;
+    p->cc_init_pixel_y = -1;
+    p->cc_init_pixel_z = -1;
+    p->alpha = (p->a0 + p->b0) / 2.;
+    p->auto_extract_conn_comp = 0;
+    p->auto_extract_conn_comp_freq = 0;
+    p->cc_binary_output = 1;
+    p->cc_init_variables = 1;
 }
 
 #define IM3D_ENTRY(...)                \
@@ -1638,6 +1816,22 @@ int im3d_gauss_filter_f64(im3d_ctx* ctx, const double* in, double* out, int nx, 
                           int pixel_approach)
 {
     IM3D_ENTRY(gauss_filter<double>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
+}
+
+int im3d_connected_component_f32(im3d_ctx* ctx, const float* img, float* res, int nx, int ny,
+                                 int nz, const float* init, int i, int j, int k, double threshold,
+                                 int full_connected, int binary_output, int* passes)
+{
+    IM3D_ENTRY(connected_component_op<float>(ctx, img, res, nx, ny, nz, init, i, j, k, threshold,
+                                             full_connected, binary_output, passes));
+}
+
+int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, int nx, int ny,
+                                 int nz, const double* init, int i, int j, int k, double threshold,
+                                 int full_connected, int binary_output, int* passes)
+{
+    IM3D_ENTRY(connected_component_op<double>(ctx, img, res, nx, ny, nz, init, i, j, k, threshold,
+                                              full_connected, binary_output, passes));
 }
 
 int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,

@@ -1802,6 +1802,116 @@ __global__ void minmax_kernel(const T* __restrict__ p, long long n, unsigned lon
     }
 }
 
+// ---- connected component (image3d<T>::connected_component, image3d_imp.hxx:1694-2120) ----
+// One byte per cell: bit 1 = white in the black-and-white image (img >= pivot, or
+// img < pivot in the negative image), bit 0 = in the component.
+
+// im_to_black_and_white (image3d_imp.hxx:1592-1623) and the initial component: the
+// cells where init != 0 and white (init != NULL), else only cell `seed` (>= 0).
+template <typename T>
+__global__ void cc_init_kernel(const T* __restrict__ img, const T* __restrict__ init,
+                               unsigned char* __restrict__ m, long long n, T pivot, int negative,
+                               long long seed)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const bool below = img[q] < pivot;
+        const unsigned char white = (unsigned char)(negative ? below : !below);
+        const unsigned char in = init ? (unsigned char)(init[q] != T(0) && white)
+                                      : (unsigned char)(q == seed);
+        m[q] = (unsigned char)((white << 1) | in);
+    }
+}
+
+// One growth pass over tiles of 32 (k) x 8 (j) x 4 (i) cells. A tile and its one-cell
+// halo are read from `in`; inside the tile the component grows to a local fixed point
+// (a white cell joins when a neighbour in the component lies off the volume's faces:
+// 1 <= i <= nx-2, 1 <= j <= ny-2 and, unless nz == 1, 1 <= k <= nz-2; 6 face
+// neighbours, 26 with FULL), then the tile is written to `out` and *changed is raised
+// if it grew. Growth only turns cells on, so passes repeated until nothing changes
+// reach the reference's fixed point whatever the order.
+constexpr int kCcK = 32, kCcJ = 8, kCcI = 4;
+template <bool FULL>
+__global__ void __launch_bounds__(256) cc_grow_kernel(const unsigned char* __restrict__ in,
+                                                      unsigned char* __restrict__ out, Dims d,
+                                                      unsigned long long* changed)
+{
+    constexpr int SK = kCcK + 2, SJ = kCcJ + 2, SI = kCcI + 2;
+    __shared__ unsigned char tile[SI * SJ * SK];
+    volatile unsigned char* t = tile;
+    const int k0 = blockIdx.x * kCcK, j0 = blockIdx.y * kCcJ, i0 = blockIdx.z * kCcI;
+    const int tid = threadIdx.y * kCcK + threadIdx.x;
+    for (int e = tid; e < SI * SJ * SK; e += 256) {
+        const int li = e / (SJ * SK), r = e - li * SJ * SK, lj = r / SK, lk = r - lj * SK;
+        const int i = i0 - 1 + li, j = j0 - 1 + lj, k = k0 - 1 + lk;
+        unsigned char v = 0;
+        if (i >= 0 && i < d.nx && j >= 0 && j < d.ny && k >= 0 && k < d.nz) v = in[d.idx(i, j, k)];
+        t[e] = v;
+    }
+    __syncthreads();
+    const int lk = threadIdx.x + 1, lj = threadIdx.y + 1;
+    const int k = k0 + threadIdx.x, j = j0 + threadIdx.y;
+    auto spreads = [&](int i, int jj, int kk) {
+        return i >= 1 && i <= d.nx - 2 && jj >= 1 && jj <= d.ny - 2 &&
+               (d.nz == 1 || (kk >= 1 && kk <= d.nz - 2));
+    };
+    bool grew = false;
+    bool step;
+    do {
+        step = false;
+#pragma unroll
+        for (int c = 0; c < kCcI; ++c) {
+            const int li = c + 1;
+            const int at = (li * SJ + lj) * SK + lk;
+            if (t[at] != 2) continue;  // only white cells not yet in the component
+            bool join = false;
+#pragma unroll
+            for (int di = -1; di <= 1; ++di)
+#pragma unroll
+                for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+                    for (int dk = -1; dk <= 1; ++dk) {
+                        const int nnz = (di != 0) + (dj != 0) + (dk != 0);
+                        if (nnz == 0 || (!FULL && nnz != 1)) continue;
+                        const int nb = ((li + di) * SJ + lj + dj) * SK + lk + dk;
+                        if ((t[nb] & 1) && spreads(i0 + c + di, j + dj, k + dk)) join = true;
+                    }
+            if (join) {
+                t[at] = 3;
+                step = true;
+                grew = true;
+            }
+        }
+    } while (__syncthreads_or(step));
+    if (k < d.nz && j < d.ny) {
+#pragma unroll
+        for (int c = 0; c < kCcI; ++c) {
+            const int i = i0 + c;
+            if (i < d.nx) out[d.idx(i, j, k)] = t[((c + 1) * SJ + lj) * SK + lk];
+        }
+    }
+    if (__syncthreads_or(grew) && tid == 0) atomicOr(changed, 1ull);
+}
+
+// The result: the component as 0 / 1, or with binary == 0 cc_not_binary_output
+// (image3d_imp.hxx:1801-1817): (res + [img < pivot]) * (img - mn) + mn.
+template <typename T>
+__global__ void cc_output_kernel(const unsigned char* __restrict__ m, const T* __restrict__ img,
+                                 T* __restrict__ res, long long n, int binary, T mn, T pivot)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        T v = (T)(m[q] & 1);
+        if (!binary) {
+            const T x = img[q];
+            v += (T)(x < pivot ? 1 : 0);
+            v *= x - mn;
+            v += mn;
+        }
+        res[q] = v;
+    }
+}
+
 // change_range_of_intensity(max, min) (image3d_imp.hxx:1628-1636) once the minimum
 // mn and the shifted maximum are known: x -= mn; x /= s; x += lo
 template <typename T>

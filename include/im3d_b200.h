@@ -79,11 +79,26 @@ typedef struct im3d_rsfe_params {
     int32_t ls_steps;           /* sweeps per outer iteration (5) */
     int32_t bc;                 /* IM3D_BC_* (IM3D_BC_DEFAULT) */
     int32_t gaussian_pixel_approach; /* build the Gaussian with unit spacing (0) */
-    int32_t init_variables;     /* reset b and div(d-b) after the first iteration (0) */
+    int32_t init_variables;     /* the first iteration resets b and div(d-b) instead of the
+                                   Bregman update: the reference's private flag, which starts
+                                   false and which an extraction raises (0) */
     int32_t sweep;              /* IM3D_SWEEP_* used by the ls_steps sweeps (LEXICOGRAPHIC) */
     int32_t gs_max_sweeps;      /* sweep cap of the residual solve (1000) */
     int32_t gs_check_every;     /* residual every this many sweeps; 0 = predicted from the
                                    observed contraction rate (0) */
+    /* automatic connected-component extraction inside the loop: the automatic case of
+     * extract_connected_component (rsfe_splitbregman_imp.hxx:448-536), run after cut_phi
+     * at every outer iteration t with t % auto_extract_conn_comp_freq == 0 (:1809) */
+    double cc_init_pixel_x;     /* seed in physical coordinates, cell floor(x / hx) (-1) */
+    double cc_init_pixel_y;     /* (-1) */
+    double cc_init_pixel_z;     /* (-1) */
+    double alpha;               /* level of phi whose inside is white: the black-and-white
+                                   threshold is (alpha - a0) / (b0 - a0) ((a0 + b0) / 2) */
+    int32_t auto_extract_conn_comp;      /* extraction on (0) */
+    int32_t auto_extract_conn_comp_freq; /* every this many outer iterations, 0 = never (0) */
+    int32_t cc_binary_output;   /* phi becomes the 0/1 component (1) or keeps its values on
+                                   the component and outside the threshold (0) */
+    int32_t cc_init_variables;  /* reset b and div(d-b) after an extraction (1) */
 } im3d_rsfe_params;
 
 typedef struct im3d_rsfe_stats {
@@ -201,6 +216,29 @@ int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, i
                         int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
                         double* phi_out, double* u_out, double* f1_out, double* f2_out,
                         im3d_rsfe_stats* stats);
+
+/* Connected component of the thresholded image, as
+ * image3d<T>::connected_component (image3d_imp.hxx:1694-2120):
+ *  - init == NULL: the component containing cell (i, j, k) (:1694-1758). The seed is
+ *    moved off the faces (to 1..dim-2; k = 0 when nz == 1); if the image is below
+ *    the pivot there, the component is taken in the negative black-and-white image.
+ *  - init != NULL: the cells connected to the cells where init != 0 and the image is
+ *    at or above the pivot (:1761-1798); i, j, k are ignored.
+ * The black-and-white image is 1 where img >= pivot = min + (max - min) * threshold
+ * (im_to_black_and_white, :1592-1623; a threshold outside [0, 1] becomes 0.5, as in
+ * the reference, and the WARNING is left in im3d_ctx_last_error with status OK).
+ * Only cells off the faces spread the component (to their 6 face neighbours, 26 with
+ * full_connected; 4 / 8 in 2-D). res receives 1 on the component and 0 elsewhere,
+ * or, with binary_output == 0, cc_not_binary_output (:1801-1817):
+ * (res + negative b&w) * (img - min) + min. img, init and res are device or host
+ * buffers in the image3d layout; nx, ny >= 2 and nz >= 1. `passes` (may be NULL)
+ * receives the number of whole-volume propagation passes run. */
+int im3d_connected_component_f32(im3d_ctx* ctx, const float* img, float* res, int nx, int ny,
+                                 int nz, const float* init, int i, int j, int k, double threshold,
+                                 int full_connected, int binary_output, int* passes);
+int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, int nx, int ny,
+                                 int nz, const double* init, int i, int j, int k, double threshold,
+                                 int full_connected, int binary_output, int* passes);
 
 /* A batch of independent volumes (BASELINE's uneven-volume workload). No counterpart
  * in the reference, which segments one image per apply(). Each descriptor holds the

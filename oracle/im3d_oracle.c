@@ -418,6 +418,146 @@ static double vmax(const double* a, size_t n)
 }
 
 /* rsfe_splitbregman<T>::apply(myim, init) (rsfe_splitbregman_imp.hxx:1547-1995). */
+/* ------------------------------------------------------------ connected component */
+
+/* image3d<T>::im_to_black_and_white (image3d_imp.hxx:1592-1623): 1 where the image is
+ * at or above pivot = min + (max - min) * threshold (0 with `negative`), a threshold
+ * outside [0, 1] replaced by 0.5. Returns the pivot. */
+double orc_im_to_bw(const double* img, size_t n, double threshold, int negative,
+                    unsigned char* bw)
+{
+    if (threshold > 1 || threshold < 0) threshold = 0.5;
+    const double mx = vmax(img, n), mn = vmin(img, n);
+    const double pivot = mn + (mx - mn) * threshold;
+    for (size_t q = 0; q < n; ++q) bw[q] = img[q] < pivot ? (unsigned char)(negative != 0)
+                                                          : (unsigned char)(negative == 0);
+    return pivot;
+}
+
+/* The growth loop of connected_component (image3d_imp.hxx:1821-2120). The reference
+ * repeats eight octant sweeps (four in 2-D) in which every set cell with
+ * 1 <= i <= nx-2, 1 <= j <= ny-2 and (nz == 1 or 1 <= k <= nz-2) copies bw into its
+ * forward face neighbours (and, with full_connected, the forward edge and corner
+ * neighbours of that octant), until a sweep changes nothing. The set cells always lie
+ * inside bw, so a copy only turns cells on, and the fixed point is the set of bw
+ * cells reachable from the initial cells through cells off the faces: 6-connected
+ * (4 in 2-D), or 26-connected (8) with full_connected. This computes that fixed point
+ * with a work list. */
+void orc_cc_grow(unsigned char* res, const unsigned char* bw, int nx, int ny, int nz, int full)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    size_t* list = (size_t*)malloc((n + 1) * sizeof(size_t));
+    size_t head = 0, tail = 0;
+    const int two_d = nz == 1;
+#define SPREADS(i, j, k) ((i) >= 1 && (i) <= nx - 2 && (j) >= 1 && (j) <= ny - 2 && \
+                          (two_d || ((k) >= 1 && (k) <= nz - 2)))
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k)
+                if (res[IDX(i, j, k)] && SPREADS(i, j, k)) list[tail++] = IDX(i, j, k);
+    while (head < tail) {
+        const size_t c = list[head++];
+        const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((size_t)nz * ny));
+        for (int di = -1; di <= 1; ++di)
+            for (int dj = -1; dj <= 1; ++dj)
+                for (int dk = (two_d ? 0 : -1); dk <= (two_d ? 0 : 1); ++dk) {
+                    const int nz_ = (di != 0) + (dj != 0) + (dk != 0);
+                    if (nz_ == 0 || (!full && nz_ != 1)) continue;
+                    const int a = i + di, b = j + dj, e = k + dk;
+                    const size_t q = IDX(a, b, e);
+                    if (res[q] || !bw[q]) continue;
+                    res[q] = 1;
+                    if (SPREADS(a, b, e)) list[tail++] = q;
+                }
+    }
+#undef SPREADS
+    free(list);
+}
+
+/* image3d<T>::connected_component (image3d_imp.hxx:1694-1817): seeded by cell
+ * (i, j, k) moved off the faces (:1700-1736; in the negative image when the seed is
+ * below the pivot, :1740-1745) when init == NULL, else by init != 0 inside bw
+ * (:1761-1798); then the growth above, and with binary_output == 0
+ * cc_not_binary_output (:1801-1817). */
+int orc_connected_component(const double* img, double* res, int nx, int ny, int nz,
+                            const double* init, int i, int j, int k, double threshold,
+                            int full_connected, int binary_output)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    unsigned char* bw = (unsigned char*)malloc(n);
+    unsigned char* r = (unsigned char*)calloc(n, 1);
+    orc_im_to_bw(img, n, threshold, 0, bw);
+    if (!init) {
+        unsigned I = (unsigned)i, J = (unsigned)j, K = (unsigned)k;
+        if (I == 0) ++I;
+        if (J == 0) ++J;
+        if (I >= (unsigned)nx - 1) I = nx - 2;
+        if (J >= (unsigned)ny - 1) J = ny - 2;
+        if (nz == 1) {
+            K = 0;
+        } else {
+            if (K == 0) ++K;
+            if (K >= (unsigned)nz - 1) K = nz - 2;
+        }
+        if (bw[IDX(I, J, K)] == 0) orc_im_to_bw(img, n, threshold, 1, bw);
+        r[IDX(I, J, K)] = 1;
+    } else {
+        for (size_t q = 0; q < n; ++q) r[q] = (unsigned char)(init[q] != 0 && bw[q]);
+    }
+    orc_cc_grow(r, bw, nx, ny, nz, full_connected);
+    for (size_t q = 0; q < n; ++q) res[q] = (double)r[q];
+    if (!binary_output) {
+        const double mn = vmin(img, n);
+        orc_im_to_bw(img, n, threshold, 1, bw);
+        for (size_t q = 0; q < n; ++q) {
+            double v = res[q];
+            v += (double)bw[q];
+            v *= img[q] - mn;
+            v += mn;
+            res[q] = v;
+        }
+    }
+    free(bw);
+    free(r);
+    return IM3D_OK;
+}
+
+/* extract_connected_component, automatic case (rsfe_splitbregman_imp.hxx:448-536):
+ * seed cell floor(cc_init_pixel / h); nothing happens when it is outside the volume or
+ * below the (alpha - a0)/(b0 - a0) threshold of phi; otherwise phi becomes its
+ * connected component (threshold 0.5, face connectivity), rescaled to [a0, b0] by
+ * change_range_of_intensity(b0, a0). Returns 1 when phi was replaced. */
+static int extract_cc(double* phi, int nx, int ny, int nz, double hx, double hy, double hz,
+                      const im3d_rsfe_params* p)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    const int i = (int)floor(p->cc_init_pixel_x / hx);
+    const int j = (int)floor(p->cc_init_pixel_y / hy);
+    const int k = (int)floor(p->cc_init_pixel_z / hz);
+    if (i < 0 || j < 0 || (nz != 1 && k < 0)) return 0;
+    const unsigned I = (unsigned)i, J = (unsigned)j, K = (unsigned)k;
+    if (I > (unsigned)nx - 1 || J > (unsigned)ny - 1 || (nz != 1 && K > (unsigned)nz - 1)) return 0;
+    unsigned char* bw = (unsigned char*)malloc(n);
+    orc_im_to_bw(phi, n, (p->alpha - p->a0) / (p->b0 - p->a0), 0, bw);
+    const int white = bw[IDX(I, J, K)] != 0;
+    free(bw);
+    if (!white) return 0;
+    double* cc = (double*)malloc(n * sizeof(double));
+    orc_connected_component(phi, cc, nx, ny, nz, NULL, (int)I, (int)J, (int)K, 0.5, 0,
+                            p->cc_binary_output);
+    /* phi = cc; change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636) */
+    const double mn = vmin(cc, n);
+    for (size_t q = 0; q < n; ++q) cc[q] -= mn;
+    const double sc = vmax(cc, n) / (p->b0 - p->a0);
+    for (size_t q = 0; q < n; ++q) {
+        cc[q] /= sc;
+        cc[q] += p->a0;
+    }
+    memcpy(phi, cc, n * sizeof(double));
+    free(cc);
+    return 1;
+}
+
 int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz, double hx,
                    double hy, double hz, const im3d_rsfe_params* p, double* phi_out,
                    double* u_out, double* f1_out, double* f2_out, im3d_rsfe_stats* stats)
@@ -582,6 +722,11 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
         for (size_t q = 0; q < n; ++q) {
             if (phi[q] < a0) phi[q] = a0;
             else if (phi[q] > b0) phi[q] = b0;
+        }
+        /* automatic connected-component extraction (:1809-1812) */
+        if (p->auto_extract_conn_comp && p->auto_extract_conn_comp_freq != 0 &&
+            t % p->auto_extract_conn_comp_freq == 0) {
+            if (extract_cc(phi, nx, ny, nz, hx, hy, hz, p) && p->cc_init_variables) init_variables = 1;
         }
         /* tolerance (:1832): normL2(phi - phiold)/normL2(phiold) */
         tollerance = sqrt(hx * hy * hz * sum_sq_diff(phi, phiold, n, nx)) /

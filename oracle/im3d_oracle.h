@@ -13,6 +13,8 @@
 #ifndef IM3D_ORACLE_H
 #define IM3D_ORACLE_H
 
+#include <stddef.h>
+
 #include "../include/im3d_b200.h"
 
 #ifdef __cplusplus
@@ -34,6 +36,12 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
                       double hz, double dt, double bc, int bc_type, double rel_res_tol,
                       int max_sweeps, int check_every, double omega, int* sweeps_done,
                       double* rel_res);
+double orc_im_to_bw(const double* img, size_t n, double threshold, int negative,
+                    unsigned char* bw);
+void orc_cc_grow(unsigned char* res, const unsigned char* bw, int nx, int ny, int nz, int full);
+int orc_connected_component(const double* img, double* res, int nx, int ny, int nz,
+                            const double* init, int i, int j, int k, double threshold,
+                            int full_connected, int binary_output);
 int orc_rsfe_apply(const double* myim, const double* init, int nx, int ny, int nz, double hx,
                    double hy, double hz, const im3d_rsfe_params* p, double* phi_out,
                    double* u_out, double* f1_out, double* f2_out, im3d_rsfe_stats* stats);

@@ -39,6 +39,10 @@ class RsfeParams(C.Structure):
         ("maxiter", C.c_int32), ("ls_steps", C.c_int32), ("bc", C.c_int32),
         ("gaussian_pixel_approach", C.c_int32), ("init_variables", C.c_int32),
         ("sweep", C.c_int32), ("gs_max_sweeps", C.c_int32), ("gs_check_every", C.c_int32),
+        ("cc_init_pixel_x", C.c_double), ("cc_init_pixel_y", C.c_double),
+        ("cc_init_pixel_z", C.c_double), ("alpha", C.c_double),
+        ("auto_extract_conn_comp", C.c_int32), ("auto_extract_conn_comp_freq", C.c_int32),
+        ("cc_binary_output", C.c_int32), ("cc_init_variables", C.c_int32),
     ]
 
 
@@ -59,7 +63,10 @@ def default_params(**kw) -> RsfeParams:
                    nu=1.0, dt=1.0, epsilon=1e-3, a0=0.0, b0=1.0, ls_tol=0.0,
                    edge_detector_sigma=0.0, gs_rel_res_tol=0.0, omega=1.0, maxiter=100,
                    ls_steps=5, bc=BC_DEFAULT, gaussian_pixel_approach=0, init_variables=0,
-                   sweep=SWEEP_LEX, gs_max_sweeps=1000, gs_check_every=0)
+                   sweep=SWEEP_LEX, gs_max_sweeps=1000, gs_check_every=0,
+                   cc_init_pixel_x=-1.0, cc_init_pixel_y=-1.0, cc_init_pixel_z=-1.0, alpha=0.5,
+                   auto_extract_conn_comp=0, auto_extract_conn_comp_freq=0, cc_binary_output=1,
+                   cc_init_variables=1)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -174,6 +181,18 @@ def rsfe_apply(myim, init=None, params=None, h=(1.0, 1.0, 1.0), use_reference=Fa
     if rc != 0:
         raise RuntimeError(f"rsfe_apply failed with status {rc}")
     return dict(phi=phi, u=u, f1=f1, f2=f2, stats={f: getattr(st, f) for f, _ in st._fields_})
+
+
+def connected_component(img, ijk=(0, 0, 0), init=None, threshold=0.5, full_connected=False,
+                        binary_output=True, use_reference=False):
+    """image3d<double>::connected_component (seeded when init is None)."""
+    x = _f64(img)
+    out = np.empty_like(x)
+    ini = None if init is None else _f64(init)
+    lib = ref_lib().ref_connected_component if use_reference else oracle_lib().orc_connected_component
+    lib(_p(x), _p(out), *map(C.c_int, x.shape), _p(ini), *map(C.c_int, ijk), C.c_double(threshold),
+        C.c_int(int(full_connected)), C.c_int(int(binary_output)))
+    return out
 
 
 # -------------------------------------------------------------- reference entry

@@ -173,6 +173,29 @@ int ref_gauss_filter_direct (const double* in, double* out, int nx, int ny, int 
     return 0;
 }
 
+/* image3d<double>::connected_component: the seeded overload (image3d_imp.hxx:1694-1758)
+ * when init == NULL, else the overload taking an initial image (:1761-1798) */
+int ref_connected_component (const double* in, double* out, int nx, int ny, int nz,
+                             const double* init, int i, int j, int k, double threshold,
+                             int full_connected, int binary_output)
+{
+    img f, r;
+    to_img (f, in, nx, ny, nz, 1., 1., 1.);
+    if (init)
+    {
+        img s;
+        to_img (s, init, nx, ny, nz, 1., 1., 1.);
+        f.connected_component (r, s, threshold, full_connected != 0, binary_output != 0);
+    }
+    else
+    {
+        f.connected_component (r, (uint) i, (uint) j, (uint) k, threshold, full_connected != 0,
+                               binary_output != 0);
+    }
+    from_img (out, r);
+    return 0;
+}
+
 /* the FFTW shim itself, for checking it against numpy.fft */
 int ref_fft3d (const double* in_interleaved, double* out_interleaved, int n0, int n1, int n2,
                int sign)
@@ -279,7 +302,15 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     algo.set_ls_tol (solve_mode ? 0 : p->ls_tol);
     algo.set_edge_detector_sigma (p->edge_detector_sigma);
     algo.set_gaussian_pixel_approach (p->gaussian_pixel_approach != 0);
-    algo.set_cc_init_variables (p->init_variables != 0);
+    // automatic connected-component extraction (public setters, :903-1022, 1380-1415)
+    algo.set_alpha (p->alpha);
+    algo.set_auto_extract_conn_comp (p->auto_extract_conn_comp != 0);
+    algo.set_auto_extract_conn_comp_freq ( (uint) p->auto_extract_conn_comp_freq);
+    if (p->cc_init_pixel_x >= 0) algo.set_cc_init_pixel_x (p->cc_init_pixel_x);
+    if (p->cc_init_pixel_y >= 0) algo.set_cc_init_pixel_y (p->cc_init_pixel_y);
+    if (p->cc_init_pixel_z >= 0) algo.set_cc_init_pixel_z (p->cc_init_pixel_z);
+    algo.set_cc_binary_output (p->cc_binary_output != 0);
+    algo.set_cc_init_variables (p->cc_init_variables != 0);
     // bc_type is private to the class (rsfe_splitbregman.hxx:108); its values are
     // NEU = 1, DIR = 2, and set_bc takes it by value, so the call goes through
     // the parameter's own type.

@@ -44,6 +44,15 @@ def ops():
     out["gs_b"] = b
     out["gs_dir"] = O.ref_gs(r0, b, dt=0.7, bc=0.3, neu=False, sweeps=3, h=ANISO)
     out["gs_neu"] = O.ref_gs(r0, b, dt=0.7, bc=0.3, neu=True, sweeps=3, h=ANISO)
+    c = rng.random((10, 9, 8))
+    out["cc_x"] = c
+    out["cc_seeded"] = O.connected_component(c, (4, 4, 4), use_reference=True)
+    out["cc_seeded_full_nonbinary"] = O.connected_component(c, (2, 3, 5), full_connected=True,
+                                                           binary_output=False,
+                                                           use_reference=True)
+    init = (rng.random((10, 9, 8)) < 0.05).astype(np.float64)
+    out["cc_init"] = init
+    out["cc_from_init"] = O.connected_component(c, init=init, threshold=0.4, use_reference=True)
     np.savez_compressed(os.path.join(HERE, "ops_f64.npz"), **out)
 
 
@@ -52,6 +61,9 @@ RSFE_MODES = {
     "dir": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2),
     "neu": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1),
     "default": dict(maxiter=4),
+    "cc": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2,
+               auto_extract_conn_comp=1, auto_extract_conn_comp_freq=2, cc_init_pixel_x=9.0,
+               cc_init_pixel_y=8.0, cc_init_pixel_z=7.0),
 }
 
 

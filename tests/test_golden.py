@@ -20,6 +20,9 @@ MODES = {
     "dir": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2),
     "neu": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1),
     "default": dict(maxiter=4),
+    "cc": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2,
+               auto_extract_conn_comp=1, auto_extract_conn_comp_freq=2, cc_init_pixel_x=9.0,
+               cc_init_pixel_y=8.0, cc_init_pixel_z=7.0),
 }
 
 
@@ -45,6 +48,12 @@ def test_oracle_ops_match_golden(O, ops):
         got = O.poisson_sweeps(ops["gs_r0"], ops["gs_b"], dt=0.7, bc=0.3, bc_type=bct, sweeps=3,
                                h=ANISO)
         assert np.array_equal(got, ops[name]), name
+    assert np.array_equal(O.connected_component(ops["cc_x"], (4, 4, 4)), ops["cc_seeded"])
+    assert np.array_equal(O.connected_component(ops["cc_x"], (2, 3, 5), full_connected=True,
+                                                binary_output=False),
+                          ops["cc_seeded_full_nonbinary"])
+    assert np.array_equal(O.connected_component(ops["cc_x"], init=ops["cc_init"], threshold=0.4),
+                          ops["cc_from_init"])
 
 
 @pytest.mark.parametrize("mode", list(MODES))
@@ -70,6 +79,12 @@ def test_gpu_ops_match_golden(ctx, ops):
         got = ctx.poisson_sweeps(ops["gs_r0"].copy(), ops["gs_b"], dt=0.7, bc=0.3, bc_type=bct,
                                  sweeps=3, h=ANISO)
         assert np.array_equal(got, ops[name]), name
+    assert np.array_equal(ctx.connected_component(ops["cc_x"], (4, 4, 4)), ops["cc_seeded"])
+    assert np.array_equal(ctx.connected_component(ops["cc_x"], (2, 3, 5), full_connected=True,
+                                                  binary_output=False),
+                          ops["cc_seeded_full_nonbinary"])
+    assert np.array_equal(ctx.connected_component(ops["cc_x"], init=ops["cc_init"], threshold=0.4),
+                          ops["cc_from_init"])
 
 
 @pytest.mark.gpu
