@@ -563,10 +563,21 @@ template <typename T>
 int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, int use_self,
              double omega)
 {
+    // the b_eff solve (no own value, omega 1) gets instantiations without the unused
+    // paths; with Dirichlet conditions and FP32 it fits 8 blocks per SM
+    const bool self = use_self || omega != 1.0;
+    const dim3 grid = grid_vec_pk<T>(d, kBlkVec);
     for (int color = 0; color < 2; ++color) {
         const int pf = prof_begin(ctx, "rb_half");
-        rb_half_vec_kernel<T, kNV><<<grid_vec_pk<T>(d, kBlkVec), kBlkVec, 0, ctx->stream>>>(
-            U, B, d, c, color, use_self, (T)omega);
+        if (self)
+            rb_half_vec_kernel<T, kNV, true, true><<<grid, kBlkVec, 0, ctx->stream>>>(
+                U, B, d, c, color, use_self, (T)omega);
+        else if (c.neu)
+            rb_half_vec_kernel<T, kNV, false, true><<<grid, kBlkVec, 0, ctx->stream>>>(
+                U, B, d, c, color, 0, T(1));
+        else
+            rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1>
+                <<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, color, 0, T(1));
         prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "rb_half"));
     }

@@ -886,11 +886,14 @@ __global__ void __launch_bounds__(256) rb_half_col_kernel(T* __restrict__ U,
 // All points of a packed row share the parity of k, so their k neighbours are the
 // other colour at (m-1, m) (k even) or (m, m+1) (k odd): one 16-byte vector plus one
 // scalar. The i neighbours come from a register window of vectors along i.
-template <typename T, int NI>
-__global__ void __launch_bounds__(256) rb_half_vec_kernel(T* __restrict__ U,
-                                                          const T* __restrict__ B, Dims d,
-                                                          GsCoef<T> c, int color, int use_self,
-                                                          T omega)
+// SELF: the point's own old value is read (use_self or omega != 1); the Poisson solve
+// on b_eff needs neither. NEU: the Neumann boundary rule is compiled in (c.neu must
+// match). Without both the kernel needs fewer registers and fits MINB blocks per SM.
+template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ U,
+                                                                const T* __restrict__ B, Dims d,
+                                                                GsCoef<T> c, int color,
+                                                                int use_self, T omega)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -908,8 +911,13 @@ __global__ void __launch_bounds__(256) rb_half_vec_kernel(T* __restrict__ U,
     const T* bb = B + (color ? npk : 0);
     const bool jint = j >= 1 && j <= d.ny - 2;
     const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
-    const bool relax = omega != T(1);
-    VV o[NI + 2];
+    const bool relax = SELF && omega != T(1);
+    if (!SELF) use_self = 0;
+    // Every load of the NI planes is issued before the first store: the stores go to
+    // the same array, so loads placed after one could not be moved ahead of it and each
+    // thread would pay one memory round trip per plane.
+    VV o[NI + 2], ymv[NI], ypv[NI], bvv[NI], sfv[NI];
+    T exv[NI];
 #pragma unroll
     for (int t = 0; t < NI + 2; ++t) {
         const int i = i0 - 1 + t;
@@ -919,20 +927,33 @@ __global__ void __launch_bounds__(256) rb_half_vec_kernel(T* __restrict__ U,
 #pragma unroll
     for (int t = 0; t < NI; ++t) {
         const int i = i0 + t;
+        const long long q = q0 + (long long)t * plane;
+        const int par = (i + j + color) & 1;
+        ymv[t] = ypv[t] = bvv[t] = sfv[t] = VV{};
+        exv[t] = T(0);
+        if (jint && i >= 1 && i <= d.nx - 2) {
+            ymv[t] = *reinterpret_cast<const VV*>(oth + q - hz);
+            ypv[t] = *reinterpret_cast<const VV*>(oth + q + hz);
+            bvv[t] = *reinterpret_cast<const VV*>(bb + q);
+            // the k neighbour not in the centre vector: m0-1 (k even) or m0+W (k odd)
+            const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
+            if (e_ok) exv[t] = oth[par ? q + W : q - 1];
+            if (SELF && (use_self || relax)) sfv[t] = *reinterpret_cast<const VV*>(own + q);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
         if (i >= d.nx) break;
         const long long q = q0 + (long long)t * plane;
         const int par = (i + j + color) & 1;
         const bool rowint = jint && i >= 1 && i <= d.nx - 2;
         if (rowint) {
-            const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
-            const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
-            const VV bv = *reinterpret_cast<const VV*>(bb + q);
-            // the k neighbour not in the centre vector: m0-1 (k even) or m0+W (k odd)
-            const long long qe = par ? q + W : q - 1;
-            const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
-            const T extra = e_ok ? oth[qe] : T(0);
-            VV self = VV{};
-            if (use_self || relax) self = *reinterpret_cast<const VV*>(own + q);
+            const VV ym = ymv[t];
+            const VV yp = ypv[t];
+            const VV bv = bvv[t];
+            const T extra = exv[t];
+            const VV self = sfv[t];
             VV outv = self;
             bool all = true;
 #pragma unroll
@@ -974,7 +995,7 @@ __global__ void __launch_bounds__(256) rb_half_vec_kernel(T* __restrict__ U,
                 }
             }
         }
-        if (c.neu) {
+        if (NEU && c.neu) {
             // Neumann: boundary points (faces of i, j or k) through the generic rule
 #pragma unroll
             for (int cc = 0; cc < W; ++cc) {

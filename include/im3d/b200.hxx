@@ -86,6 +86,12 @@ struct ops<float>
         return im3d_rsfe_apply_f32 (c, u0, init, x, y, z, hx, hy, hz, p, phi, nullptr, nullptr,
                                     nullptr, st);
     }
+    static int cc (im3d_ctx* c, float const* img, float* res, int x, int y, int z,
+                   float const* init, int i, int j, int k, double thr, int full, int bin)
+    {
+        return im3d_connected_component_f32 (c, img, res, x, y, z, init, i, j, k, thr, full, bin,
+                                             nullptr);
+    }
 };
 
 template <>
@@ -118,6 +124,12 @@ struct ops<double>
     {
         return im3d_rsfe_apply_f64 (c, u0, init, x, y, z, hx, hy, hz, p, phi, nullptr, nullptr,
                                     nullptr, st);
+    }
+    static int cc (im3d_ctx* c, double const* img, double* res, int x, int y, int z,
+                   double const* init, int i, int j, int k, double thr, int full, int bin)
+    {
+        return im3d_connected_component_f64 (c, img, res, x, y, z, init, i, j, k, thr, full, bin,
+                                             nullptr);
     }
 };
 

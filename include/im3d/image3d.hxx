@@ -194,12 +194,71 @@ public:
         }
     }
 
+    // black and white image (image3d_imp.hxx:1592-1623): 1 where the image is at or
+    // above min + (max - min) * threshold, 0 elsewhere (the other way round if negative)
+    template <typename S>
+    void im_to_black_and_white (image3d<S>& res, double threshold = 0.5,
+                                bool negative = false) const
+    {
+        if (threshold > 1 || threshold < 0)
+        {
+            std::cout << "WARNING::im_to_black_and_white: threshold must be between 0 and 1, ";
+            std::cout << "otherwise default value 0.5 is applied" << std::endl;
+            threshold = 0.5;
+        }
+        const T mx (this->max() ), mn (this->min() ), pivot (mn + (mx - mn) * threshold);
+        res.setdim (dimx, dimy, dimz);
+        res.seth (hx, hy, hz);
+        for (size_t q = 0; q < rawimage.size(); ++q)
+            res.rawimage[q] = static_cast<S> (rawimage[q] < pivot ? int (negative) : 1 - int (negative) );
+    }
+
+    // ---- connected components on the B200 backend (image3d_imp.hxx:1694-2120)
+    // the component containing cell (i, j, k) of the black and white image
+    template <typename S>
+    void connected_component (image3d<S>& res, uint const& i, uint const& j, uint const& k,
+                              double threshold = 0.5, bool full_connected = false,
+                              bool binary_output = true) const
+    {
+        cc_backend (res, nullptr, (int) i, (int) j, (int) k, threshold, full_connected, binary_output);
+    }
+
+    // the cells connected to the non-zero cells of init that are white
+    template <typename S>
+    void connected_component (image3d<S>& res, image3d<S> const& init, double threshold = 0.5,
+                              bool full_connected = false, bool binary_output = true) const
+    {
+        if (init.getdimx() != dimx || init.getdimy() != dimy || init.getdimz() != dimz)
+        {
+            std::cout << "WARNING: in image3d::connected_component: dimensions of init must be ";
+            std::cout << "the same of the image" << std::endl;
+            return;
+        }
+        std::vector<T> ini (rawimage.size() );
+        for (size_t q = 0; q < ini.size(); ++q) ini[q] = static_cast<T> (init.rawimage[q] != S (0) );
+        cc_backend (res, ini.data(), 0, 0, 0, threshold, full_connected, binary_output);
+    }
+
     template <typename S, typename R>
     friend void vector_abs (image3d<S>& res, std::vector<image3d<R> > const& fun);
     template <typename S, typename R>
     friend void div (image3d<S>& res, std::vector<image3d<R> > const& fun);
 
 private:
+    template <typename S>
+    void cc_backend (image3d<S>& res, T const* init, int i, int j, int k, double threshold,
+                     bool full_connected, bool binary_output) const
+    {
+        std::vector<T> out (rawimage.size() );
+        if (b200::failed (b200::ops<T>::cc (b200::context(), rawimage.data(), out.data(), dimx, dimy,
+                                            dimz, init, i, j, k, threshold, full_connected ? 1 : 0,
+                                            binary_output ? 1 : 0), "image3d::connected_component") )
+            return;
+        res.setdim (dimx, dimy, dimz);
+        res.seth (hx, hy, hz);
+        for (size_t q = 0; q < out.size(); ++q) res.rawimage[q] = static_cast<S> (out[q]);
+    }
+
     void reset (T const& value)
     {
         rawimage.assign ( (size_t) dimx * dimy * dimz, value);

@@ -14,9 +14,13 @@
  * sweep). Any other function pointer cannot run inside the GPU loop: apply() prints a
  * WARNING and uses the default of its kind.
  *
- * Not on this backend: interactive display (showfrequency, on-the-go updates),
- * connected-component extraction, per-iteration dumps (dumpfrequency writes only the
- * final level set, "<outputname>_<t>_final"), 2-D images.
+ * The automatic connected-component extraction (auto_extract_conn_comp with
+ * auto_extract_conn_comp_freq and a cc_init_pixel seed, imp :448-536) runs on the GPU
+ * inside the loop.
+ *
+ * Not on this backend: interactive display (showfrequency, on-the-go updates) and the
+ * interactive choice of a connected component, per-iteration dumps (dumpfrequency
+ * writes only the final level set, "<outputname>_<t>_final"), 2-D images.
  */
 #ifndef IM3D_RSFE_SPLITBREGMAN_HXX
 #define IM3D_RSFE_SPLITBREGMAN_HXX
@@ -360,9 +364,9 @@ private:
         std::clog << "- dimensions:\t" << dimx << " x " << dimy << " x " << dimz << std::endl;
         std::clog << "- spacing:\t" << myim.gethx() << " x " << myim.gethy() << " x "
                   << myim.gethz() << std::endl;
-        if (showfrequency || auto_extract_conn_comp)
-            std::clog << "WARNING::apply: display and connected-component extraction are not "
-                      << "part of the B200 backend" << std::endl;
+        if (showfrequency)
+            std::clog << "WARNING::apply: display (and the interactive connected-component "
+                      << "choice) is not part of the B200 backend" << std::endl;
         auto cvf = cv.function();
         if (cvf != &conv::acyclic_fftw_convolution<T> && cvf != &conv::direct_convolution<T>)
             std::clog << "WARNING::apply: custom convolution not supported by the B200 backend, "
@@ -393,6 +397,14 @@ private:
         p.gs_rel_res_tol = gs_rel_res_tol;
         p.omega = omega;
         p.gs_max_sweeps = gs_max_sweeps;
+        p.alpha = this->alpha;
+        p.auto_extract_conn_comp = auto_extract_conn_comp ? 1 : 0;
+        p.auto_extract_conn_comp_freq = (int32_t) auto_extract_conn_comp_freq;
+        p.cc_init_pixel_x = cc_init_pixel_x;
+        p.cc_init_pixel_y = cc_init_pixel_y;
+        p.cc_init_pixel_z = cc_init_pixel_z;
+        p.cc_binary_output = cc_binary_output ? 1 : 0;
+        p.cc_init_variables = cc_init_variables ? 1 : 0;
 
         std::vector<T> full;
         T const* ini = nullptr;

@@ -105,5 +105,28 @@ int main (int argc, char** argv)
     algo.apply (u0, init);
     im3d::interface<double> (algo.getoutput() ).write (dir + "/phi_out");
     std::cout << "iterations " << algo.get_stats().iterations << std::endl;
+
+    // connected component of the read volume, and black & white conversion
+    im3d::image3d<double> cc, bw;
+    u0.connected_component (cc, 10, 9, 8, 0.5, true);
+    im3d::interface<double> (cc).write (dir + "/cc_out");
+    u0.im_to_black_and_white (bw, 0.5);
+    const double pivot = u0.min() + (u0.max() - u0.min() ) * 0.5;
+    bool bw_ok = true;
+    for (size_t q = 0; q < bw.size(); ++q)
+        bw_ok = bw_ok && bw.data() [q] == (u0.data() [q] < pivot ? 0. : 1.);
+    check (bw_ok, "im_to_black_and_white");
+
+    // the loop with the automatic connected-component extraction
+    segm::rsfe_splitbregman<double> algo2;
+    algo2.set_verbosity (false);
+    algo2.set_getpotfile (dir + "/params.pot");
+    algo2.set_auto_extract_conn_comp (true);
+    algo2.set_auto_extract_conn_comp_freq (2);
+    algo2.set_cc_init_pixel_x (10);
+    algo2.set_cc_init_pixel_y (9);
+    algo2.set_cc_init_pixel_z (8);
+    algo2.apply (u0, init);
+    im3d::interface<double> (algo2.getoutput() ).write (dir + "/phi_cc_out");
     return failures ? 1 : 0;
 }

@@ -80,6 +80,14 @@ def test_cpp_api_on_gpu(tmp_path, pkg, O):
     want = O.rsfe_apply(u0, phi0, O.default_params(maxiter=6, sigma=2.0, lamda=0.5, lamda1=1.0,
                                                    lamda2=1.0, bc=O.BC_DIR, ls_steps=1, tol=0.0))
     assert rel(phi, want["phi"]) < 1e-9
+    cc, _ = mhd.read(str(tmp_path / "cc_out.mhd"))
+    assert np.array_equal(cc, O.connected_component(u0, (10, 9, 8), full_connected=True))
+    phi_cc, _ = mhd.read(str(tmp_path / "phi_cc_out.mhd"))
+    want = O.rsfe_apply(u0, phi0, O.default_params(
+        maxiter=6, sigma=2.0, lamda=0.5, lamda1=1.0, lamda2=1.0, bc=O.BC_DIR, ls_steps=1, tol=0.0,
+        auto_extract_conn_comp=1, auto_extract_conn_comp_freq=2, cc_init_pixel_x=10.0,
+        cc_init_pixel_y=9.0, cc_init_pixel_z=8.0))
+    assert rel(phi_cc, want["phi"]) < 1e-9
 
 
 @pytest.mark.gpu
