@@ -45,10 +45,16 @@ __device__ __forceinline__ void heaviside_pair(T phi, T center, T inv_eps, T& H,
 }
 
 // ------------------------------------------------------------ loaders/storers
+// A loader's raw() issues the memory reads of one cell and cook() turns them into the
+// staged fields, so that a pass can issue the reads of all its cells before it
+// computes any of them; operator() does both.
 template <typename T, int N>
 struct LdVec {
     const Vec<T, N>* p;
     Dims d;
+    typedef Vec<T, N> Raw;
+    __device__ __forceinline__ Raw raw(int i, int j, int k) const { return p[d.idx(i, j, k)]; }
+    __device__ __forceinline__ Vec<T, N> cook(const Raw& r) const { return r; }
     __device__ __forceinline__ Vec<T, N> operator()(int i, int j, int k) const
     {
         return p[d.idx(i, j, k)];
@@ -69,6 +75,9 @@ template <typename T>
 struct LdScalar {
     const T* p;
     Dims d;
+    typedef Vec<T, 1> Raw;
+    __device__ __forceinline__ Raw raw(int i, int j, int k) const { return (*this)(i, j, k); }
+    __device__ __forceinline__ Vec<T, 1> cook(const Raw& r) const { return r; }
     __device__ __forceinline__ Vec<T, 1> operator()(int i, int j, int k) const
     {
         Vec<T, 1> r;
@@ -79,6 +88,9 @@ struct LdScalar {
 
 template <typename T>
 struct LdOne {
+    typedef Vec<T, 1> Raw;
+    __device__ __forceinline__ Raw raw(int i, int j, int k) const { return (*this)(i, j, k); }
+    __device__ __forceinline__ Vec<T, 1> cook(const Raw& r) const { return r; }
     __device__ __forceinline__ Vec<T, 1> operator()(int, int, int) const
     {
         Vec<T, 1> r;
@@ -104,19 +116,26 @@ struct LdHeaviside {
     const T* u0;
     Dims d;
     T center, inv_eps;
-    __device__ __forceinline__ Vec<T, 4> operator()(int i, int j, int k) const
+    struct Raw {
+        T phi, u;
+    };
+    __device__ __forceinline__ Raw raw(int i, int j, int k) const
     {
         const long long q = d.idx(i, j, k);
+        return Raw{ld_g(phi + q), ld_g(u0 + q)};
+    }
+    __device__ __forceinline__ Vec<T, 4> cook(const Raw& w) const
+    {
         T H, Hb;
-        heaviside_pair(ld_g(phi + q), center, inv_eps, H, Hb);
-        const T u = ld_g(u0 + q);
+        heaviside_pair(w.phi, center, inv_eps, H, Hb);
         Vec<T, 4> r;
-        r.v[0] = H * u;
+        r.v[0] = H * w.u;
         r.v[1] = H;
-        r.v[2] = Hb * u;
+        r.v[2] = Hb * w.u;
         r.v[3] = Hb;
         return r;
     }
+    __device__ __forceinline__ Vec<T, 4> operator()(int i, int j, int k) const { return cook(raw(i, j, k)); }
 };
 
 // Forcing term of the Poisson step (rsfe_splitbregman_imp.hxx:1750-1761), from
@@ -298,13 +317,19 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     const int k0 = blockIdx.y * TK;
     {
         constexpr int NL = (W + TKT - 1) / TKT;
-        Vec<T, N> v[NL];
+        // all reads first, then the loader's arithmetic (the Heaviside for stage 1)
+        typename Ld::Raw rw[NL];
+        bool ok[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.x + u * TKT;
             const int k = k0 - SP + s;
-            v[u] = (s < W && live && k >= 0 && k < d.nz) ? ld(i, j, k) : vzero<T, N>();
+            ok[u] = s < W && live && k >= 0 && k < d.nz;
+            if (ok[u]) rw[u] = ld.raw(i, j, k);
         }
+        Vec<T, N> v[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) v[u] = ok[u] ? ld.cook(rw[u]) : vzero<T, N>();
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.x + u * TKT;
