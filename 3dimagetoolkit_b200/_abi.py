@@ -69,11 +69,11 @@ class RsfeStats(C.Structure):
         ("last_tol", C.c_double), ("last_rel_res", C.c_double), ("last_ls_err", C.c_double),
         ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_sweeps", C.c_int64),
         ("iterations", C.c_int32), ("last_sweeps", C.c_int32), ("not_converged", C.c_int32),
-        ("reserved", C.c_int32),
+        ("residual_checks", C.c_int32),
     ]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class VolumeDesc(C.Structure):

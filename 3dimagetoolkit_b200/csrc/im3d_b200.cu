@@ -63,6 +63,7 @@ struct im3d_ctx {
     bool tb_enabled = false;
     int pair_resident[2] = {0, 0};  // resident rb_pair_kernel CTAs (24- and 22-row tiles)
     int num_sms = 148;
+    long long residual_checks = 0;  // rb_check calls, for the statistics
 };
 
 namespace {
@@ -600,15 +601,21 @@ int finalize(im3d_ctx* ctx, const double* part, dim3 grid, int nvals, int slot)
 }
 
 // Next residual check of the Poisson solve. check_every > 0: a fixed interval.
-// check_every == 0: first checks after 4 and 8 sweeps, then the remaining sweeps are
-// predicted from the contraction between the last two checks,
-//   rate = (r_s / r_prev)^(1/(s - s_prev)),  need = log(tol / r_s) / log(rate),
-// and the next check is ceil(need) sweeps later, clamped to [1, 32].
-int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every)
+// Otherwise the remaining sweeps are predicted from the contraction rate,
+//   need = log(tol / r_s) / log(rate),
+// and the next check is ceil(need) sweeps later, clamped to [1, 32]. The rate is
+// (r_s / r_prev)^(1/(s - s_prev)) once two residuals of this solve are known, else the
+// rate carried over from the previous solve (rate_hint in (0, 1)), else the next
+// check is 4 sweeps later. *rate_used receives the rate a prediction used.
+int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every,
+               double rate_hint, double* rate_used)
 {
     if (check_every > 0) return s + check_every;
-    if (s_prev <= 0 || !(r_prev > r_s) || !(r_s > 0)) return s + 4;
-    const double rate = std::pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    double rate;
+    if (s_prev > 0 && r_prev > r_s && r_s > 0) rate = std::pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    else if (rate_hint > 0 && rate_hint < 1 && r_s > 0) rate = rate_hint;
+    else return s + 4;
+    *rate_used = rate;
     const double need = std::log(tol / r_s) / std::log(rate);
     int step = 32;
     if (need == need && need < 32.0) step = (int)std::ceil(need);
@@ -730,6 +737,7 @@ int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<
     const int nvals = *beff2 < 0 ? 2 : 1;
     double* part = nullptr;
     IM3D_TRY(part_buf(ctx, grid, nvals, &part));
+    ctx->residual_checks++;
     const int pf = prof_begin(ctx, "rb_residual");
     rb_residual_vec_kernel<T, kNV><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
     prof_end(ctx, pf);
@@ -743,17 +751,22 @@ int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<
 }
 
 // Red-black solve on the packed layout (U holds u_in on entry, B = b_eff packed).
-// Residual every check_every sweeps; sum b_eff^2 is taken on the first check.
+// Residual on the schedule of next_check, the first one after first_check sweeps
+// (0: after 4); sum b_eff^2 is taken on the first check. *rate_out (may be NULL)
+// receives the last contraction rate the schedule used (rate_hint if none), so that
+// the next solve of a segmentation can start from it.
 template <typename T>
 int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, double tol,
-             int max_sweeps, int check_every, double omega, int* sweeps, double* rel, bool* conv)
+             int max_sweeps, int check_every, double omega, int* sweeps, double* rel, bool* conv,
+             int first_check = 0, double rate_hint = 0, double* rate_out = nullptr)
 {
     if (check_every < 0) check_every = 0;
     if (max_sweeps < 1) max_sweeps = 1;
     double beff2 = -1;
     int s = 0, s_prev = 0;
-    double r_prev = -1;
-    int next = check_every > 0 ? check_every : 4;
+    double r_prev = -1, rate_used = 0;
+    int next = check_every > 0 ? check_every : (first_check > 0 ? first_check : 4);
+    if (rate_out) *rate_out = rate_hint;
     *conv = false;
     *rel = -1;
     l2_pin(ctx, U, 2 * (size_t)d.npk() * sizeof(T));
@@ -784,11 +797,12 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
                     done = true;
                     break;
                 }
-                next = next_check(s, r, s_prev, r_prev, tol, check_every);
+                next = next_check(s, r, s_prev, r_prev, tol, check_every, rate_hint, &rate_used);
                 if (next > max_sweeps) next = max_sweeps;
                 s_prev = s;
                 r_prev = r;
             }
+            if (rate_out) *rate_out = rate_used > 0 ? rate_used : rate_hint;
             if (cur != U)
                 IM3D_CUDA(ctx, cudaMemcpyAsync(U, cur, cnt * sizeof(T), cudaMemcpyDeviceToDevice,
                                                ctx->stream));
@@ -809,12 +823,13 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
                 *conv = true;
                 break;
             }
-            next = next_check(s, r, s_prev, r_prev, tol, check_every);
+            next = next_check(s, r, s_prev, r_prev, tol, check_every, rate_hint, &rate_used);
             if (next > max_sweeps) next = max_sweeps;
             s_prev = s;
             r_prev = r;
         }
     }
+    if (rate_out) *rate_out = rate_used > 0 ? rate_used : rate_hint;
     *sweeps = s;
     return IM3D_OK;
 }
@@ -1104,6 +1119,9 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     int init_variables = p->init_variables;
     long long total_sweeps = 0;
     int last_sweeps = 0, not_conv = 0, t;
+    int sched_first = 0;  // residual schedule carried between Poisson solves
+    const long long checks0 = ctx->residual_checks;
+    double sched_rate = 0;
     double last_rel = -1, last_ls_err = -1;
     T* phi = phiA;   // current level set (natural)
     T* other = phiB;
@@ -1140,8 +1158,15 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             int sw = 0;
             double rel = -1;
             bool conv = false;
+            // each solve's residual schedule starts from the previous one: the first
+            // check after as many sweeps as it needed, its contraction rate as the first
+            // prediction (the sweep counts of consecutive solves differ by a sweep or two)
+            double rate = 0;
             IM3D_TRY(rb_solve<T>(ctx, upk, bpk, d, coef, p->gs_rel_res_tol, p->gs_max_sweeps,
-                                 p->gs_check_every, p->omega, &sw, &rel, &conv));
+                                 p->gs_check_every, p->omega, &sw, &rel, &conv, sched_first,
+                                 sched_rate, &rate));
+            sched_first = conv ? sw : 0;
+            sched_rate = conv ? rate : 0;
             if (!conv) not_conv++;
             total_sweeps += sw;
             last_sweeps = sw;
@@ -1280,6 +1305,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         stats->last_rel_res = last_rel;
         stats->last_ls_err = last_ls_err;
         stats->not_converged = not_conv;
+        stats->residual_checks = (int32_t)(ctx->residual_checks - checks0);
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
         stats->setup_ms = ms;

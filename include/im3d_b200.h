@@ -111,7 +111,7 @@ typedef struct im3d_rsfe_stats {
     int32_t iterations;   /* outer iterations run */
     int32_t last_sweeps;  /* sweeps of the last outer iteration */
     int32_t not_converged;/* outer iterations whose solve hit gs_max_sweeps */
-    int32_t reserved;
+    int32_t residual_checks; /* residual evaluations of the Poisson solves (residual mode) */
 } im3d_rsfe_stats;
 
 typedef struct im3d_ctx im3d_ctx;

@@ -315,14 +315,19 @@ static void solve_residual(const gs_geom* g, const double* u, const double* uin,
     *bb = sb;
 }
 
-/* Next residual check: a fixed interval when check_every > 0; otherwise first
- * checks after 4 and 8 sweeps, then ceil(log(tol/r_s)/log(rate)) sweeps later with
- * rate = (r_s/r_prev)^(1/(s - s_prev)), clamped to [1, 32]. */
-static int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every)
+/* Next residual check: a fixed interval when check_every > 0; otherwise
+ * ceil(log(tol/r_s)/log(rate)) sweeps later, clamped to [1, 32], with
+ * rate = (r_s/r_prev)^(1/(s - s_prev)) once two residuals are known, else the rate
+ * carried over from the previous solve (rate_hint in (0, 1)), else 4 sweeps later. */
+static int next_check(int s, double r_s, int s_prev, double r_prev, double tol, int check_every,
+                      double rate_hint, double* rate_used)
 {
     if (check_every > 0) return s + check_every;
-    if (s_prev <= 0 || !(r_prev > r_s) || !(r_s > 0)) return s + 4;
-    double rate = pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    double rate;
+    if (s_prev > 0 && r_prev > r_s && r_s > 0) rate = pow(r_s / r_prev, 1.0 / (double)(s - s_prev));
+    else if (rate_hint > 0 && rate_hint < 1 && r_s > 0) rate = rate_hint;
+    else return s + 4;
+    *rate_used = rate;
     double need = log(tol / r_s) / log(rate);
     int step = 32;
     if (need == need && need < 32.0) step = (int)ceil(need);
@@ -332,11 +337,14 @@ static int next_check(int s, double r_s, int s_prev, double r_prev, double tol, 
 
 /* Red-black solve of (1/dt - Lap) u = uin/dt + b with uin = u on entry held fixed
  * (the converged form of one unsteady step; the reference's single sweep is its
- * first Gauss-Seidel iterate). Residual checked on the schedule of next_check. */
-int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double hx, double hy,
-                      double hz, double dt, double bc, int bc_type, double rel_res_tol,
-                      int max_sweeps, int check_every, double omega, int* sweeps_done,
-                      double* rel_res)
+ * first Gauss-Seidel iterate). Residual checked on the schedule of next_check; the
+ * first check comes after first_check sweeps (0: after 4). rate_out (may be NULL)
+ * receives the last contraction rate the schedule used (rate_hint if none). */
+int orc_poisson_solve_sched(double* u, const double* b, int nx, int ny, int nz, double hx,
+                            double hy, double hz, double dt, double bc, int bc_type,
+                            double rel_res_tol, int max_sweeps, int check_every, double omega,
+                            int first_check, double rate_hint, int* sweeps_done,
+                            double* rel_res, double* rate_out, int* checks)
 {
     gs_geom g;
     make_geom(&g, nx, ny, nz, hx, hy, hz, dt, bc, bc_type);
@@ -349,8 +357,8 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
     if (check_every < 0) check_every = 0;
     if (max_sweeps < 1) max_sweeps = 1;
     int s = 0, conv = 0, s_prev = 0;
-    int next = check_every > 0 ? check_every : 4;
-    double rel = -1, r_prev = -1;
+    int next = check_every > 0 ? check_every : (first_check > 0 ? first_check : 4);
+    double rel = -1, r_prev = -1, rate_used = 0;
     while (s < max_sweeps) {
         for (int color = 0; color < 2; ++color) {
             #pragma omp parallel for schedule(static)
@@ -368,9 +376,10 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
         if (s >= next || s == max_sweeps) {
             double rr, bb;
             solve_residual(&g, u, uin, b, &rr, &bb);
+            if (checks) ++*checks;
             rel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
             if (rel <= rel_res_tol) { conv = 1; break; }
-            next = next_check(s, rel, s_prev, r_prev, rel_res_tol, check_every);
+            next = next_check(s, rel, s_prev, r_prev, rel_res_tol, check_every, rate_hint, &rate_used);
             if (next > max_sweeps) next = max_sweeps;
             s_prev = s;
             r_prev = rel;
@@ -379,7 +388,18 @@ int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double
     free(uin);
     if (sweeps_done) *sweeps_done = s;
     if (rel_res) *rel_res = rel;
+    if (rate_out) *rate_out = rate_used > 0 ? rate_used : rate_hint;
     return conv ? IM3D_OK : IM3D_ERR_NOT_CONVERGED;
+}
+
+int orc_poisson_solve(double* u, const double* b, int nx, int ny, int nz, double hx, double hy,
+                      double hz, double dt, double bc, int bc_type, double rel_res_tol,
+                      int max_sweeps, int check_every, double omega, int* sweeps_done,
+                      double* rel_res)
+{
+    return orc_poisson_solve_sched(u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
+                                   max_sweeps, check_every, omega, 0, 0.0, sweeps_done, rel_res,
+                                   NULL, NULL);
 }
 
 /* ------------------------------------------------------------------- the loop */
@@ -642,6 +662,9 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
     /* chosen_bc (:1735-1743): NEU -> 0, DIR -> a0; the constructor default is NEU */
     const double chosen_bc = (bc_type == IM3D_BC_DIR) ? a0 : 0.;
     const int neu = bc_type == IM3D_BC_NEU;
+    int sched_first = 0;     /* residual schedule carried between Poisson solves */
+    int checks = 0;
+    double sched_rate = 0;
 
     for (t = 1; tollerance > p->tol && t <= p->maxiter; ++t) {
         memcpy(phiold, phi, n * sizeof(double));
@@ -694,10 +717,16 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
         /* the Poisson step (:1768-1785) */
         if (p->gs_rel_res_tol > 0) {
             int sw = 0;
-            double rel = -1;
-            int st = orc_poisson_solve(phi, kr2, nx, ny, nz, hx, hy, hz, p->dt, chosen_bc,
-                                       neu ? IM3D_BC_NEU : IM3D_BC_DIR, p->gs_rel_res_tol,
-                                       p->gs_max_sweeps, p->gs_check_every, p->omega, &sw, &rel);
+            double rel = -1, rate = 0;
+            /* the schedule of each solve starts from the previous one: first check
+             * after as many sweeps as it needed, its contraction rate as the first
+             * prediction */
+            int st = orc_poisson_solve_sched(phi, kr2, nx, ny, nz, hx, hy, hz, p->dt, chosen_bc,
+                                             neu ? IM3D_BC_NEU : IM3D_BC_DIR, p->gs_rel_res_tol,
+                                             p->gs_max_sweeps, p->gs_check_every, p->omega,
+                                             sched_first, sched_rate, &sw, &rel, &rate, &checks);
+            sched_first = st == IM3D_OK ? sw : 0;
+            sched_rate = st == IM3D_OK ? rate : 0;
             if (st != IM3D_OK) not_conv++;
             total_sweeps += sw;
             last_sweeps = sw;
@@ -763,6 +792,7 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
         stats->last_rel_res = last_rel;
         stats->last_ls_err = last_ls_err;
         stats->not_converged = not_conv;
+        stats->residual_checks = checks;
     }
     free(phiold); free(kones); free(kmyim); free(g); free(divdb); free(bb); free(d);
     free(num); free(den); free(f1); free(f2); free(kr1); free(kr2); free(aux);

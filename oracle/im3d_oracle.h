@@ -42,6 +42,11 @@ void orc_cc_grow(unsigned char* res, const unsigned char* bw, int nx, int ny, in
 int orc_connected_component(const double* img, double* res, int nx, int ny, int nz,
                             const double* init, int i, int j, int k, double threshold,
                             int full_connected, int binary_output);
+int orc_poisson_solve_sched(double* u, const double* b, int nx, int ny, int nz, double hx,
+                            double hy, double hz, double dt, double bc, int bc_type,
+                            double rel_res_tol, int max_sweeps, int check_every, double omega,
+                            int first_check, double rate_hint, int* sweeps_done,
+                            double* rel_res, double* rate_out, int* checks);
 int orc_rsfe_apply(const double* myim, const double* init, int nx, int ny, int nz, double hx,
                    double hy, double hz, const im3d_rsfe_params* p, double* phi_out,
                    double* u_out, double* f1_out, double* f2_out, im3d_rsfe_stats* stats);

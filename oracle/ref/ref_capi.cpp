@@ -58,6 +58,9 @@ struct Recorder
     int bc_type = IM3D_BC_DIR;
     double rel_res_tol = 0, omega = 1;
     int max_sweeps = 1000, check_every = 0;
+    int sched_first = 0;
+    double sched_rate = 0;
+    int checks = 0;
     long long sweeps = 0;
     int last_sweeps = 0;
     double last_rel = -1;
@@ -125,11 +128,15 @@ void rec_poisson (img& res, img const& b, double const& dt, double const& bc, im
         else
         {
             int sw = 0;
-            double rel = -1;
-            int st = orc_poisson_solve (r.data(), bb.data(), nx, ny, nz, res.gethx(), res.gethy(),
-                                        res.gethz(), dt, bc, g_rec.bc_type, g_rec.rel_res_tol,
-                                        g_rec.max_sweeps, g_rec.check_every, g_rec.omega, &sw,
-                                        &rel);
+            double rel = -1, rate = 0;
+            // the residual schedule carries over from the previous solve of this apply
+            int st = orc_poisson_solve_sched (r.data(), bb.data(), nx, ny, nz, res.gethx(),
+                                              res.gethy(), res.gethz(), dt, bc, g_rec.bc_type,
+                                              g_rec.rel_res_tol, g_rec.max_sweeps,
+                                              g_rec.check_every, g_rec.omega, g_rec.sched_first,
+                                              g_rec.sched_rate, &sw, &rel, &rate, &g_rec.checks);
+            g_rec.sched_first = st == IM3D_OK ? sw : 0;
+            g_rec.sched_rate = st == IM3D_OK ? rate : 0;
             if (st != IM3D_OK) g_rec.not_converged++;
             g_rec.sweeps += sw;
             g_rec.last_sweeps = sw;
@@ -370,6 +377,7 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
         stats->last_sweeps = g_rec.last_sweeps;
         stats->last_rel_res = g_rec.last_rel;
         stats->not_converged = g_rec.not_converged;
+        stats->residual_checks = g_rec.checks;
     }
     g_rec = Recorder();
     return 0;

@@ -81,6 +81,7 @@ def test_full_loop_restatement_vs_reference(O, pkg, mode):
         assert rel(a[key], b[key]) < 1e-12, key
     assert a["stats"]["iterations"] == b["stats"]["iterations"] == 5
     assert a["stats"]["total_sweeps"] == b["stats"]["total_sweeps"]
+    assert a["stats"]["residual_checks"] == b["stats"]["residual_checks"]
 
 
 def test_known_answers_of_reference_examples(O):
