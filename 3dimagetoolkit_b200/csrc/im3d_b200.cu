@@ -560,6 +560,26 @@ dim3 grid_col(const Dims& d, dim3 blk)
     return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNI - 1) / kNI);
 }
 
+// Launch as a programmatic dependent of the previous kernel on the stream: the kernel
+// must begin with griddepcontrol.wait (rb_half_vec_kernel does), which holds it until
+// the previous grid's writes are visible.
+template <typename... KArgs, typename... Args>
+int launch_dependent(im3d_ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 blk, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = blk;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    IM3D_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+    return IM3D_OK;
+}
+
 template <typename T>
 int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, int use_self,
              double omega)
@@ -571,14 +591,14 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
     for (int color = 0; color < 2; ++color) {
         const int pf = prof_begin(ctx, "rb_half");
         if (self)
-            rb_half_vec_kernel<T, kNV, true, true><<<grid, kBlkVec, 0, ctx->stream>>>(
-                U, B, d, c, color, use_self, (T)omega);
+            IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, true, true>, grid, kBlkVec, U,
+                                      B, d, c, color, use_self, (T)omega));
         else if (c.neu)
-            rb_half_vec_kernel<T, kNV, false, true><<<grid, kBlkVec, 0, ctx->stream>>>(
-                U, B, d, c, color, 0, T(1));
+            IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, true>, grid, kBlkVec,
+                                      U, B, d, c, color, 0, T(1)));
         else
-            rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1>
-                <<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, color, 0, T(1));
+            IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1>,
+                                      grid, kBlkVec, U, B, d, c, color, 0, T(1)));
         prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "rb_half"));
     }

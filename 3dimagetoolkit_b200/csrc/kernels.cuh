@@ -923,6 +923,11 @@ __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ 
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
+    // Launched as a programmatic dependent of the previous half-sweep: wait until its
+    // writes are visible, then let the next half-sweep's blocks be scheduled while this
+    // one drains (both are no-ops in an ordinary launch).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i0 = blockIdx.z * NI;
