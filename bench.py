@@ -140,6 +140,32 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- GPU arm
+def half_sweep_us(ctx, shape, dev, stream):
+    """Device time of one red-black half-sweep inside a Poisson solve, in us."""
+    import torch
+
+    with torch.cuda.stream(stream):  # every tensor op ordered with the library's launches
+        g = torch.Generator(device=dev)
+        g.manual_seed(11)
+        u = torch.rand(shape, device=dev, dtype=torch.float32, generator=g)
+        b = torch.rand(shape, device=dev, dtype=torch.float32, generator=g) - 0.5
+
+        def solve_ms(sweeps):
+            uu = u.clone()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.poisson_solve(uu, b, bc_type=2, tol=0.0, max_sweeps=sweeps, check_every=sweeps)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        solve_ms(2)
+        solve_ms(202)
+        d = sorted(solve_ms(202) - solve_ms(2) for _ in range(3))
+    return d[1] * 1000.0 / 400.0
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -260,12 +286,21 @@ def run_gpu(args):
     prof = ctx.profile(reset=True)
     ctx.set_profiling(False)
 
+    # the half-sweep in its real launch sequence: per-launch events break the overlap of
+    # consecutive (programmatically dependent) sweeps, so the dominant kernel is also
+    # timed as the difference of a 202- and a 2-sweep solve on the same stream
+    # (400 half-sweeps back to back; each solve has one residual check)
+    sweep_us = half_sweep_us(ctx, shape, dev, stream) if rank == 0 else None
+
     result = None
     if rank == 0:
         peak, peak_kind = peaks()
         top = max(prof.items(), key=lambda kv: kv[1][0])
         name, (ms_total, count) = top
         avg_s = ms_total / count * 1e-3
+        avg_s_events = avg_s
+        if name == "rb_half" and sweep_us:
+            avg_s = sweep_us * 1e-6
         per_vox = ALGO_BYTES_PER_VOXEL.get(name)
         achieved = per_vox * n / avg_s / 1e9 if per_vox else None
         traffic = None
@@ -280,6 +315,10 @@ def run_gpu(args):
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
             "algo_bytes_per_launch": per_vox * n if per_vox else None,
             "avg_launch_us": avg_s * 1e6, "launches_per_step": count,
+            "avg_launch_us_events": avg_s_events * 1e6,
+            "launch_timing": ("back-to-back launches inside one solve (202- minus 2-sweep solve, "
+                              "CUDA events on the library's stream)" if avg_s != avg_s_events
+                              else "CUDA events around each launch in a profiled pass"),
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)",
             "share_of_step": ms_total / prof_total if prof_total else None,
         }
