@@ -590,15 +590,18 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
     const dim3 grid = grid_vec_pk<T>(d, kBlkVec);
     for (int color = 0; color < 2; ++color) {
         const int pf = prof_begin(ctx, "rb_half");
+        // red walks the planes forward, black backward: each half-sweep starts on the
+        // planes the previous one wrote last, which are still in L2
+        const int reverse = color;
         if (self)
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, true, true>, grid, kBlkVec, U,
-                                      B, d, c, color, use_self, (T)omega));
+                                      B, d, c, color, use_self, (T)omega, reverse));
         else if (c.neu)
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, true>, grid, kBlkVec,
-                                      U, B, d, c, color, 0, T(1)));
+                                      U, B, d, c, color, 0, T(1), reverse));
         else
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1>,
-                                      grid, kBlkVec, U, B, d, c, color, 0, T(1)));
+                                      grid, kBlkVec, U, B, d, c, color, 0, T(1), reverse));
         prof_end(ctx, pf);
         IM3D_TRY(check_launch(ctx, "rb_half"));
     }

@@ -914,11 +914,15 @@ __global__ void __launch_bounds__(256) rb_half_col_kernel(T* __restrict__ U,
 // SELF: the point's own old value is read (use_self or omega != 1); the Poisson solve
 // on b_eff needs neither. NEU: the Neumann boundary rule is compiled in (c.neu must
 // match). Without both the kernel needs fewer registers and fits MINB blocks per SM.
+// reverse: the blocks take the planes of i from the last to the first, so that a
+// half-sweep following one in the other direction starts on the planes that are still
+// in L2.
 template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
 __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ U,
                                                                 const T* __restrict__ B, Dims d,
                                                                 GsCoef<T> c, int color,
-                                                                int use_self, T omega)
+                                                                int use_self, T omega,
+                                                                int reverse = 0)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -930,7 +934,7 @@ __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ 
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i0 = blockIdx.z * NI;
+    const int i0 = (reverse ? gridDim.z - 1 - blockIdx.z : blockIdx.z) * NI;
     const int hz = d.hz();
     const int m0 = g * W;
     if (m0 >= hz || j >= d.ny) return;
