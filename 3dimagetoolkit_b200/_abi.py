@@ -58,6 +58,7 @@ class RsfeParams(C.Structure):
         ("cc_init_pixel_z", C.c_double), ("alpha", C.c_double),
         ("auto_extract_conn_comp", C.c_int32), ("auto_extract_conn_comp_freq", C.c_int32),
         ("cc_binary_output", C.c_int32), ("cc_init_variables", C.c_int32),
+        ("conv_cyclic", C.c_int32), ("reserved_", C.c_int32),
     ]
 
     def as_dict(self):
@@ -217,11 +218,15 @@ class Context:
         self._check(lib().im3d_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 
     # -- operators -----------------------------------------------------------
-    def gauss_filter(self, x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, out=None):
+    def gauss_filter(self, x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, out=None,
+                     cyclic=False):
+        """acyclic_fftw_convolution (zero boundary) or, with cyclic, cyclic_fftw_convolution
+        (periodic boundary) with the normalised Gaussian."""
         px, dt = _ptr(x)
         out = _empty_like(x) if out is None else out
         po, _ = _ptr(out)
-        fn = getattr(lib(), "im3d_gauss_filter_" + _suffix(dt))
+        name = "im3d_gauss_filter_cyclic_" if cyclic else "im3d_gauss_filter_"
+        fn = getattr(lib(), name + _suffix(dt))
         self._check(fn(self._h, px, po, *map(C.c_int, x.shape), *map(C.c_double, h),
                        C.c_double(sigma), C.c_double(radius), C.c_int(int(pixel_approach))))
         return out

@@ -18,6 +18,23 @@ namespace im3d {
 
 struct Dims {
     int nx, ny, nz;
+    // boundary of the Gaussian convolution passes: 0 = zero outside the volume
+    // (acyclic_fftw_convolution), 1 = periodic (cyclic_fftw_convolution)
+    int cyc = 0;
+    // a halo index along an axis of length n: false when outside and the boundary is
+    // zero, else the index (wrapped into [0, n) for the periodic boundary)
+    __host__ __device__ bool halo(int a, int n, int& out) const
+    {
+        if (a >= 0 && a < n) {
+            out = a;
+            return true;
+        }
+        if (!cyc) return false;
+        int r = a % n;
+        if (r < 0) r += n;
+        out = r;
+        return true;
+    }
     __host__ __device__ long long n() const { return (long long)nx * ny * nz; }
     // packed row pitch: (nz+1)/2 points of one colour, padded to a multiple of 4 so that
     // every packed row starts 16-byte aligned (padding slots hold no point: k >= nz)

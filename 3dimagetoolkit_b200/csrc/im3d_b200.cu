@@ -1049,7 +1049,9 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         return fail(ctx, IM3D_ERR_INVALID_ARG, "omega must lie in (0, 2)");
 
     IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
-    const Dims d{nx, ny, nz};
+    // the convolution passes take the plug-in's boundary; no other kernel reads cyc
+    Dims d{nx, ny, nz};
+    d.cyc = p->conv_cyclic ? 1 : 0;
     const long long n = d.n();
     const long long npk2 = 2 * d.npk();
     const bool solve = p->gs_rel_res_tol > 0;
@@ -1341,11 +1343,13 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
 // ------------------------------------------------------ standalone operators
 template <typename T>
 int gauss_filter(im3d_ctx* ctx, const T* in_user, T* out_user, int nx, int ny, int nz, double hx,
-                 double hy, double hz, double sigma, double radius, int pixel_approach)
+                 double hy, double hz, double sigma, double radius, int pixel_approach,
+                 int cyclic = 0)
 {
     IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
     if (!in_user || !out_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "NULL volume");
-    const Dims d{nx, ny, nz};
+    Dims d{nx, ny, nz};
+    d.cyc = cyclic ? 1 : 0;
     const T* in = nullptr;
     T* out = nullptr;
     IM3D_TRY(dev_in<T>(ctx, in_user, d.n(), "in_a", &in));
@@ -1855,6 +1859,8 @@ void im3d_rsfe_params_default(im3d_rsfe_params* p)
     p->auto_extract_conn_comp_freq = 0;
     p->cc_binary_output = 1;
     p->cc_init_variables = 1;
+    p->conv_cyclic = 0;
+    p->reserved_ = 0;
 }
 
 #define IM3D_ENTRY(...)                \
@@ -1892,6 +1898,22 @@ int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, 
 {
     IM3D_ENTRY(connected_component_op<double>(ctx, img, res, nx, ny, nz, init, i, j, k, threshold,
                                               full_connected, binary_output, passes));
+}
+
+int im3d_gauss_filter_cyclic_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny,
+                                 int nz, double hx, double hy, double hz, double sigma,
+                                 double radius, int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius,
+                                   pixel_approach, 1));
+}
+
+int im3d_gauss_filter_cyclic_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny,
+                                 int nz, double hx, double hy, double hz, double sigma,
+                                 double radius, int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<double>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius,
+                                    pixel_approach, 1));
 }
 
 int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,

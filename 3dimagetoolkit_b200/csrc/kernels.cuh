@@ -226,8 +226,8 @@ __global__ void __launch_bounds__(TK* RK) conv_k_kernel(Ld ld, St st, Dims d, co
     const int k0 = blockIdx.y * TK;
     Vec<T, N>* srow = sm + threadIdx.y * W;
     for (int s = threadIdx.x; s < W; s += TK) {
-        const int k = k0 - S + s;
-        srow[s] = (live && k >= 0 && k < d.nz) ? ld(i, j, k) : vzero<T, N>();
+        int kk = 0;
+        srow[s] = (live && d.halo(k0 - S + s, d.nz, kk)) ? ld(i, j, kk) : vzero<T, N>();
     }
     __syncthreads();
     const int k = k0 + threadIdx.x;
@@ -255,9 +255,9 @@ __global__ void __launch_bounds__(TW* TY) conv_s_kernel(Ld ld, St st, Dims d, co
     const int len = AXIS == 0 ? d.nx : d.ny;
     const bool kin = k < d.nz;
     for (int s = threadIdx.y; s < H; s += TY) {
-        const int a = a0 - S + s;
+        int a = 0;
         Vec<T, N> v = vzero<T, N>();
-        if (kin && a >= 0 && a < len) v = AXIS == 0 ? ld(a, other, k) : ld(other, a, k);
+        if (kin && d.halo(a0 - S + s, len, a)) v = AXIS == 0 ? ld(a, other, k) : ld(other, a, k);
         sm[s * TW + threadIdx.x] = v;
     }
     __syncthreads();
@@ -323,8 +323,8 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.x + u * TKT;
-            const int k = k0 - SP + s;
-            ok[u] = s < W && live && k >= 0 && k < d.nz;
+            int k = 0;
+            ok[u] = s < W && live && d.halo(k0 - SP + s, d.nz, k);
             if (ok[u]) rw[u] = ld.raw(i, j, k);
         }
         Vec<T, N> v[NL];
@@ -402,9 +402,9 @@ __global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.y + u * TY;
-            const int a = a0 - S + s;
+            int a = 0;
             v[u] = vzero<T, N>();
-            if (s < H && kin && a >= 0 && a < len) v[u] = AXIS == 0 ? ld(a, other, k) : ld(other, a, k);
+            if (s < H && kin && d.halo(a0 - S + s, len, a)) v[u] = AXIS == 0 ? ld(a, other, k) : ld(other, a, k);
         }
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
@@ -468,9 +468,9 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>*
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.y + u * TY;
-            const int i = i0 - 2 * S + s;
+            int i = 0;
             v[u] = vzero<T, 4>();
-            if (s < H1 && kin && i >= 0 && i < d.nx) v[u] = in[d.idx(i, j, k)];
+            if (s < H1 && kin && d.halo(i0 - 2 * S + s, d.nx, i)) v[u] = in[d.idx(i, j, k)];
         }
 #pragma unroll
         for (int u = 0; u < NL; ++u) {
@@ -499,12 +499,15 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>*
             const int s = r0 + r;           // first-pass row: i = i0 - S + s
             const int i = i0 - S + s;
             T pv = T(0), qv = T(0);
-            if (kin && i >= 0 && i < d.nx) {
+            // rows outside the volume are zero for the second convolution, or the
+            // rows they wrap to for the periodic boundary
+            const bool inside = i >= 0 && i < d.nx;
+            if (kin && (inside || d.cyc)) {
                 const T f1 = c[0][r] / c[1][r];
                 const T f2 = c[2][r] / c[3][r];
                 pv = f1 * l1 - f2 * l2;
                 qv = (f1 * f1) * l1 - (f2 * f2) * l2;
-                if (f1_out && s >= S && s < S + TA) {
+                if (f1_out && inside && s >= S && s < S + TA) {
                     const long long qq = d.idx(i, j, k);
                     f1_out[qq] = f1;
                     f2_out[qq] = f2;
@@ -565,22 +568,23 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_kernel(const Vec<T, 4>* __r
     const int j = blockIdx.z;
     const bool kin = k < d.nz;
     for (int s = threadIdx.y; s < H1; s += TY) {
-        const int i = i0 - 2 * S + s;
+        int i = 0;
         Vec<T, 4> v = vzero<T, 4>();
-        if (kin && i >= 0 && i < d.nx) v = in[d.idx(i, j, k)];
+        if (kin && d.halo(i0 - 2 * S + s, d.nx, i)) v = in[d.idx(i, j, k)];
         sin[s * TW + threadIdx.x] = v;
     }
     __syncthreads();
     for (int s = threadIdx.y; s < H2; s += TY) {
         const int i = i0 - S + s;
         Vec<T, 2> m = vzero<T, 2>();
-        if (kin && i >= 0 && i < d.nx) {
+        const bool inside = i >= 0 && i < d.nx;
+        if (kin && (inside || d.cyc)) {
             const Vec<T, 4> c = tap_sum<T, 4>(sin + s * TW + threadIdx.x, TW, wsm, nh);
             const T f1 = c.v[0] / c.v[1];
             const T f2 = c.v[2] / c.v[3];
             m.v[0] = f1 * l1 - f2 * l2;
             m.v[1] = (f1 * f1) * l1 - (f2 * f2) * l2;
-            if (f1_out && s >= S && s < S + TA) {
+            if (f1_out && inside && s >= S && s < S + TA) {
                 const long long q = d.idx(i, j, k);
                 f1_out[q] = f1;
                 f2_out[q] = f2;

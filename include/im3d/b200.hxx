@@ -60,9 +60,10 @@ template <>
 struct ops<float>
 {
     static int gauss (im3d_ctx* c, float const* in, float* out, int x, int y, int z, double hx,
-                      double hy, double hz, double s, double r, int gpa)
+                      double hy, double hz, double s, double r, int gpa, int cyc = 0)
     {
-        return im3d_gauss_filter_f32 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa);
+        return cyc ? im3d_gauss_filter_cyclic_f32 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa)
+                   : im3d_gauss_filter_f32 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa);
     }
     static int sweeps (im3d_ctx* c, float* res, float const* b, int x, int y, int z, double hx,
                        double hy, double hz, double dt, double bc, int bct, int order, int n)
@@ -98,9 +99,10 @@ template <>
 struct ops<double>
 {
     static int gauss (im3d_ctx* c, double const* in, double* out, int x, int y, int z,
-                      double hx, double hy, double hz, double s, double r, int gpa)
+                      double hx, double hy, double hz, double s, double r, int gpa, int cyc = 0)
     {
-        return im3d_gauss_filter_f64 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa);
+        return cyc ? im3d_gauss_filter_cyclic_f64 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa)
+                   : im3d_gauss_filter_f64 (c, in, out, x, y, z, hx, hy, hz, s, r, gpa);
     }
     static int sweeps (im3d_ctx* c, double* res, double const* b, int x, int y, int z,
                        double hx, double hy, double hz, double dt, double bc, int bct, int order,

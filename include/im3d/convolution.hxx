@@ -7,9 +7,10 @@
  * and direct_convolution then filter on the GPU (im3d_gauss_filter_*). Both are the
  * same linear convolution with zero boundary in the reference
  * (convolution_imp.hxx:535-653 and :761-812); the backend evaluates it as three 1-D
- * passes of the normalised Gaussian. Filters other than the Gaussian
- * (build_high_pass_filter, build_laplacian_filter) and the periodic
- * cyclic_fftw_convolution are not part of this backend.
+ * passes of the normalised Gaussian. cyclic_fftw_convolution (:657-754) takes the
+ * volume as periodic and runs as the same passes with wrapped indices
+ * (im3d_gauss_filter_cyclic_*). Filters other than the Gaussian
+ * (build_high_pass_filter, build_laplacian_filter) are not part of this backend.
  */
 #ifndef IM3D_CONVOLUTION_HXX
 #define IM3D_CONVOLUTION_HXX
@@ -92,7 +93,8 @@ template <typename T> bool filtering<T>::pixel_approach = false;
 template <typename T> bool filtering<T>::built = false;
 
 template <typename T>
-void gaussian_gpu_filter (im3d::image3d<T>& result, im3d::image3d<T> const& factor, char const* who)
+void gaussian_gpu_filter (im3d::image3d<T>& result, im3d::image3d<T> const& factor, char const* who,
+                          bool cyclic = false)
 {
     if (!filtering<T>::built)
     {
@@ -107,7 +109,8 @@ void gaussian_gpu_filter (im3d::image3d<T>& result, im3d::image3d<T> const& fact
                                                    factor.getdimx(), factor.getdimy(), factor.getdimz(),
                                                    factor.gethx(), factor.gethy(), factor.gethz(),
                                                    filtering<T>::sigma, filtering<T>::radius,
-                                                   filtering<T>::pixel_approach ? 1 : 0), who);
+                                                   filtering<T>::pixel_approach ? 1 : 0, cyclic ? 1 : 0),
+                        who);
 }
 
 /* conv::acyclic_fftw_convolution (convolution_imp.hxx:535-653) */
@@ -115,6 +118,13 @@ template <typename T>
 void acyclic_fftw_convolution (im3d::image3d<T>& result, im3d::image3d<T> const& factor)
 {
     gaussian_gpu_filter (result, factor, "acyclic_fftw_convolution");
+}
+
+/* conv::cyclic_fftw_convolution (convolution_imp.hxx:657-754): periodic boundary */
+template <typename T>
+void cyclic_fftw_convolution (im3d::image3d<T>& result, im3d::image3d<T> const& factor)
+{
+    gaussian_gpu_filter (result, factor, "cyclic_fftw_convolution", true);
 }
 
 /* conv::direct_convolution (convolution_imp.hxx:761-812): the same linear convolution */

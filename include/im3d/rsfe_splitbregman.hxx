@@ -9,7 +9,8 @@
  *
  * Plug-ins: the functors installed with set_cv / set_onestep_poisson / set_bc are
  * recognised and mapped onto the backend: acyclic_fftw_convolution and
- * direct_convolution (the same linear Gaussian filter), DirGaussSeidel,
+ * direct_convolution (the same linear Gaussian filter), cyclic_fftw_convolution (the
+ * periodic one), DirGaussSeidel,
  * NeuGaussSeidel (the reference's lexicographic sweep) and RBGaussSeidel (a red-black
  * sweep). Any other function pointer cannot run inside the GPU loop: apply() prints a
  * WARNING and uses the default of its kind.
@@ -368,7 +369,8 @@ private:
             std::clog << "WARNING::apply: display (and the interactive connected-component "
                       << "choice) is not part of the B200 backend" << std::endl;
         auto cvf = cv.function();
-        if (cvf != &conv::acyclic_fftw_convolution<T> && cvf != &conv::direct_convolution<T>)
+        if (cvf != &conv::acyclic_fftw_convolution<T> && cvf != &conv::direct_convolution<T> &&
+                cvf != &conv::cyclic_fftw_convolution<T>)
             std::clog << "WARNING::apply: custom convolution not supported by the B200 backend, "
                       << "the Gaussian filter is used" << std::endl;
 
@@ -405,6 +407,7 @@ private:
         p.cc_init_pixel_z = cc_init_pixel_z;
         p.cc_binary_output = cc_binary_output ? 1 : 0;
         p.cc_init_variables = cc_init_variables ? 1 : 0;
+        p.conv_cyclic = cvf == &conv::cyclic_fftw_convolution<T> ? 1 : 0;
 
         std::vector<T> full;
         T const* ini = nullptr;

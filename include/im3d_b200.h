@@ -99,6 +99,11 @@ typedef struct im3d_rsfe_params {
     int32_t cc_binary_output;   /* phi becomes the 0/1 component (1) or keeps its values on
                                    the component and outside the threshold (0) */
     int32_t cc_init_variables;  /* reset b and div(d-b) after an extraction (1) */
+    /* the convolution plug-in (set_cv, rsfe_splitbregman_imp.hxx:836-842): 0 =
+     * acyclic_fftw_convolution (zero boundary, the constructor's choice), 1 =
+     * cyclic_fftw_convolution (periodic boundary) */
+    int32_t conv_cyclic;
+    int32_t reserved_;
 } im3d_rsfe_params;
 
 typedef struct im3d_rsfe_stats {
@@ -148,6 +153,18 @@ int im3d_gauss_filter_f32(im3d_ctx* ctx, const float* in, float* out, int nx, in
 int im3d_gauss_filter_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
                           double hx, double hy, double hz, double sigma, double radius,
                           int pixel_approach);
+
+/* The same Gaussian with conv::cyclic_fftw_convolution (convolution_imp.hxx:657-754,
+ * filter built by build_freq_filters' cyclic part, :406-528): the volume is taken as
+ * periodic (the reference periodises it over a grid of the volume's size, repeated
+ * until it covers the kernel), so each axis pass is the circular convolution
+ * out[a] = sum_t w[t] in[(a - t) mod n]. */
+int im3d_gauss_filter_cyclic_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny,
+                                 int nz, double hx, double hy, double hz, double sigma,
+                                 double radius, int pixel_approach);
+int im3d_gauss_filter_cyclic_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny,
+                                 int nz, double hx, double hy, double hz, double sigma,
+                                 double radius, int pixel_approach);
 
 /* `sweeps` calls of lapl::DirGaussSeidel (bc_type DIR or DEFAULT) or
  * lapl::NeuGaussSeidel (NEU), in place on res (poisson_imp.hxx:340-429, 23-336):

@@ -46,8 +46,10 @@ int orc_gauss_taps(double sigma, double radius, double h, double* taps, int cap)
     return nh;
 }
 
+/* One axis of the separable filter: zero outside the volume, or with `cyclic` the
+ * circular convolution out[a] = sum_t w[t] in[(a - t) mod len]. */
 static void conv_axis(const double* in, double* out, int nx, int ny, int nz, int axis,
-                      const double* w, int nh)
+                      const double* w, int nh, int cyclic)
 {
     const int shift = nh / 2;
     const int len = axis == 0 ? nx : (axis == 1 ? ny : nz);
@@ -61,6 +63,7 @@ static void conv_axis(const double* in, double* out, int nx, int ny, int nz, int
                 double acc = 0;
                 for (int t = 0; t < nh; ++t) {
                     int q = pos - (t - shift);
+                    if (cyclic) q = ((q % len) + len) % len;
                     if (q >= 0 && q < len) acc += w[t] * base[(size_t)q * stride];
                 }
                 out[IDX(i, j, k)] = acc;
@@ -70,8 +73,9 @@ static void conv_axis(const double* in, double* out, int nx, int ny, int nz, int
 /* build_gaussian_filter (convolution_imp.hxx:22-91) + acyclic_fftw_convolution
  * (:535-653): result = linear convolution with the normalised Gaussian, zero outside
  * the volume, cropped to [0,dim). pixel_approach uses unit spacing for the taps. */
-void orc_gauss_filter(const double* in, double* out, int nx, int ny, int nz, double hx,
-                      double hy, double hz, double sigma, double radius, int pixel_approach)
+void orc_gauss_filter_mode(const double* in, double* out, int nx, int ny, int nz, double hx,
+                           double hy, double hz, double sigma, double radius,
+                           int pixel_approach, int cyclic)
 {
     double wx[4096], wy[4096], wz[4096];
     double gx = pixel_approach ? 1. : hx, gy = pixel_approach ? 1. : hy,
@@ -82,10 +86,27 @@ void orc_gauss_filter(const double* in, double* out, int nx, int ny, int nz, dou
     if (nz == 1) wz[0] = 1.;
     size_t n = (size_t)nx * ny * nz;
     double* tmp = (double*)malloc(n * sizeof(double));
-    conv_axis(in, out, nx, ny, nz, 2, wz, nhz);
-    conv_axis(out, tmp, nx, ny, nz, 1, wy, nhy);
-    conv_axis(tmp, out, nx, ny, nz, 0, wx, nhx);
+    conv_axis(in, out, nx, ny, nz, 2, wz, nhz, cyclic);
+    conv_axis(out, tmp, nx, ny, nz, 1, wy, nhy, cyclic);
+    conv_axis(tmp, out, nx, ny, nz, 0, wx, nhx, cyclic);
     free(tmp);
+}
+
+void orc_gauss_filter(const double* in, double* out, int nx, int ny, int nz, double hx,
+                      double hy, double hz, double sigma, double radius, int pixel_approach)
+{
+    orc_gauss_filter_mode(in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach, 0);
+}
+
+/* build_gaussian_filter + cyclic_fftw_convolution (convolution_imp.hxx:406-528,
+ * 657-754): the reference periodises the volume over a grid of its own size (repeated
+ * until it covers the kernel) and multiplies by the DFT of the wrapped kernel, which
+ * is the circular convolution of each axis with the normalised taps. */
+void orc_gauss_filter_cyclic(const double* in, double* out, int nx, int ny, int nz, double hx,
+                             double hy, double hz, double sigma, double radius,
+                             int pixel_approach)
+{
+    orc_gauss_filter_mode(in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach, 1);
 }
 
 /* image3d<T>::grad, 3-D branch (image3d_imp.hxx:750-838): central differences
@@ -623,16 +644,16 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
 
     /* kones = K*1, kmyim = K*u0 (:1648-1651) */
     for (size_t q = 0; q < n; ++q) aux[q] = 1.;
-    orc_gauss_filter(aux, kones, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
-    orc_gauss_filter(u0, kmyim, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
+    orc_gauss_filter_mode(aux, kones, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
+    orc_gauss_filter_mode(u0, kmyim, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
 
     /* edge_detect, GRAD branch (:196-316): optional pre-blur, |grad u0|^2, then
      * g = nu / (lamda (1 + beta |grad u0|^2)) in the reference's operation order */
     {
         const double* src = u0;
         if (p->edge_detector_sigma != 0) {
-            orc_gauss_filter(u0, aux, nx, ny, nz, hx, hy, hz, p->edge_detector_sigma, 3,
-                             p->gaussian_pixel_approach);
+            orc_gauss_filter_mode(u0, aux, nx, ny, nz, hx, hy, hz, p->edge_detector_sigma, 3,
+                             p->gaussian_pixel_approach, p->conv_cyclic);
             src = aux;
         }
         orc_grad(src, d, nx, ny, nz, hx, hy, hz);
@@ -674,8 +695,8 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
             aux[q] = H * u0[q];
             f1[q] = H;
         }
-        orc_gauss_filter(aux, num, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
-        orc_gauss_filter(f1, den, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
+        orc_gauss_filter_mode(aux, num, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
+        orc_gauss_filter_mode(f1, den, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
         /* f1, f2 (:1709-1717) */
         for (size_t q = 0; q < n; ++q) {
             f1[q] = num[q] / den[q];
@@ -685,7 +706,7 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
         }
         /* kr2 = K*(lamda1 f1 - lamda2 f2), kr1 = K*(lamda1 f1^2 - lamda2 f2^2) (:1720-1729) */
         for (size_t q = 0; q < n; ++q) aux[q] = f1[q] * p->lamda1 - f2[q] * p->lamda2;
-        orc_gauss_filter(aux, kr2, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
+        orc_gauss_filter_mode(aux, kr2, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
         for (size_t q = 0; q < n; ++q) {
             double a = f1[q];
             a *= a;
@@ -696,7 +717,7 @@ int orc_rsfe_apply(const double* u0, const double* init, int nx, int ny, int nz,
             a -= b2;
             aux[q] = a;
         }
-        orc_gauss_filter(aux, kr1, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach);
+        orc_gauss_filter_mode(aux, kr1, nx, ny, nz, hx, hy, hz, p->sigma, 3, p->gaussian_pixel_approach, p->conv_cyclic);
         if (f1_out) memcpy(f1_out, f1, n * sizeof(double));
         if (f2_out) memcpy(f2_out, f2, n * sizeof(double));
         /* forcing term (:1750-1761) */

@@ -25,6 +25,12 @@ extern "C" {
 int orc_gauss_taps(double sigma, double radius, double h, double* taps, int cap);
 void orc_gauss_filter(const double* in, double* out, int nx, int ny, int nz, double hx,
                       double hy, double hz, double sigma, double radius, int pixel_approach);
+void orc_gauss_filter_cyclic(const double* in, double* out, int nx, int ny, int nz, double hx,
+                             double hy, double hz, double sigma, double radius,
+                             int pixel_approach);
+void orc_gauss_filter_mode(const double* in, double* out, int nx, int ny, int nz, double hx,
+                           double hy, double hz, double sigma, double radius,
+                           int pixel_approach, int cyclic);
 void orc_grad(const double* in, double* out3, int nx, int ny, int nz, double hx, double hy,
               double hz);
 void orc_div(const double* in3, double* out, int nx, int ny, int nz, double hx, double hy,

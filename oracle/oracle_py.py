@@ -43,6 +43,7 @@ class RsfeParams(C.Structure):
         ("cc_init_pixel_z", C.c_double), ("alpha", C.c_double),
         ("auto_extract_conn_comp", C.c_int32), ("auto_extract_conn_comp_freq", C.c_int32),
         ("cc_binary_output", C.c_int32), ("cc_init_variables", C.c_int32),
+        ("conv_cyclic", C.c_int32), ("reserved_", C.c_int32),
     ]
 
 
@@ -66,7 +67,7 @@ def default_params(**kw) -> RsfeParams:
                    sweep=SWEEP_LEX, gs_max_sweeps=1000, gs_check_every=0,
                    cc_init_pixel_x=-1.0, cc_init_pixel_y=-1.0, cc_init_pixel_z=-1.0, alpha=0.5,
                    auto_extract_conn_comp=0, auto_extract_conn_comp_freq=0, cc_binary_output=1,
-                   cc_init_variables=1)
+                   cc_init_variables=1, conv_cyclic=0, reserved_=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -106,11 +107,15 @@ def _f64(a):
 
 # ----------------------------------------------------------------- restatement
 
-def gauss_filter(x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, lib=None):
+def gauss_filter(x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, lib=None,
+                 cyclic=False):
     x = _f64(x)
     out = np.empty_like(x)
     L = lib or oracle_lib()
-    fn = L.orc_gauss_filter if lib is None else L.ref_gauss_filter
+    if cyclic:
+        fn = L.orc_gauss_filter_cyclic if lib is None else L.ref_gauss_filter_cyclic
+    else:
+        fn = L.orc_gauss_filter if lib is None else L.ref_gauss_filter
     fn(_p(x), _p(out), *map(C.c_int, x.shape), *map(C.c_double, h), C.c_double(sigma),
        C.c_double(radius), C.c_int(int(pixel_approach)))
     return out
@@ -198,11 +203,12 @@ def connected_component(img, ijk=(0, 0, 0), init=None, threshold=0.5, full_conne
 # -------------------------------------------------------------- reference entry
 
 def ref_gauss_filter(x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False,
-                     direct=False):
+                     direct=False, cyclic=False):
     x = _f64(x)
     out = np.empty_like(x)
     L = ref_lib()
-    fn = L.ref_gauss_filter_direct if direct else L.ref_gauss_filter
+    fn = (L.ref_gauss_filter_cyclic if cyclic else
+          (L.ref_gauss_filter_direct if direct else L.ref_gauss_filter))
     fn(_p(x), _p(out), *map(C.c_int, x.shape), *map(C.c_double, h), C.c_double(sigma),
        C.c_double(radius), C.c_int(int(pixel_approach)))
     return out

@@ -87,9 +87,22 @@ void call_with_enum (segm::rsfe_splitbregman<double>& a,
     (a.*f) (static_cast<E> (v) );
 }
 
+void record_conv (img const& result);
+
 void rec_conv (img& result, img const& factor)
 {
     conv::acyclic_fftw_convolution (result, factor);
+    record_conv (result);
+}
+
+void rec_conv_cyclic (img& result, img const& factor)
+{
+    conv::cyclic_fftw_convolution (result, factor);
+    record_conv (result);
+}
+
+void record_conv (img const& result)
+{
     const int c = g_rec.conv_calls++;
     if (c == 0) g_rec.kones = result;
     else if (c == 1) g_rec.kmyim = result;
@@ -163,6 +176,19 @@ int ref_gauss_filter (const double* in, double* out, int nx, int ny, int nz, dou
     to_img (f, in, nx, ny, nz, hx, hy, hz);
     conv::filtering<double>::build_gaussian_filter (f, sigma, radius, pixel_approach != 0);
     conv::acyclic_fftw_convolution (r, f);
+    from_img (out, r);
+    return 0;
+}
+
+/* conv::filtering<double>::build_gaussian_filter + cyclic_fftw_convolution */
+int ref_gauss_filter_cyclic (const double* in, double* out, int nx, int ny, int nz, double hx,
+                             double hy, double hz, double sigma, double radius,
+                             int pixel_approach)
+{
+    img f, r;
+    to_img (f, in, nx, ny, nz, hx, hy, hz);
+    conv::filtering<double>::build_gaussian_filter (f, sigma, radius, pixel_approach != 0);
+    conv::cyclic_fftw_convolution (r, f);
     from_img (out, r);
     return 0;
 }
@@ -325,7 +351,7 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     {
         call_with_enum (algo, &segm::rsfe_splitbregman<double>::set_bc, p->bc);
     }
-    algo.set_cv (conv::filtering<double> (rec_conv) );
+    algo.set_cv (conv::filtering<double> (p->conv_cyclic ? rec_conv_cyclic : rec_conv) );
 
     const bool neu = p->bc == IM3D_BC_NEU;
     g_rec.bc_type = neu ? IM3D_BC_NEU : IM3D_BC_DIR;

@@ -32,6 +32,7 @@ def ops():
     out["conv_x"] = x
     out["conv_iso"] = O.ref_gauss_filter(x, 2.0)
     out["conv_aniso_gpa"] = O.ref_gauss_filter(x, 1.5, h=ANISO, pixel_approach=True)
+    out["conv_cyclic"] = O.ref_gauss_filter(x, 2.0, h=ANISO, cyclic=True)
     g = rng.random((7, 9, 11))
     out["grad_x"] = g
     out["grad"] = O.ref_grad(g, ANISO)
@@ -61,6 +62,8 @@ RSFE_MODES = {
     "dir": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2),
     "neu": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1),
     "default": dict(maxiter=4),
+    "cyclic": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1,
+                   conv_cyclic=1),
     "cc": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2,
                auto_extract_conn_comp=1, auto_extract_conn_comp_freq=2, cc_init_pixel_x=9.0,
                cc_init_pixel_y=8.0, cc_init_pixel_z=7.0),

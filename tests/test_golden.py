@@ -20,6 +20,8 @@ MODES = {
     "dir": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2),
     "neu": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1),
     "default": dict(maxiter=4),
+    "cyclic": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=1,
+                   conv_cyclic=1),
     "cc": dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=6, ls_steps=1, bc=2,
                auto_extract_conn_comp=1, auto_extract_conn_comp_freq=2, cc_init_pixel_x=9.0,
                cc_init_pixel_y=8.0, cc_init_pixel_z=7.0),
@@ -42,6 +44,7 @@ def test_oracle_ops_match_golden(O, ops):
     assert rel(O.gauss_filter(ops["conv_x"], 2.0), ops["conv_iso"]) < 1e-14
     assert rel(O.gauss_filter(ops["conv_x"], 1.5, h=ANISO, pixel_approach=True),
                ops["conv_aniso_gpa"]) < 1e-14
+    assert rel(O.gauss_filter(ops["conv_x"], 2.0, h=ANISO, cyclic=True), ops["conv_cyclic"]) < 1e-14
     assert np.array_equal(O.grad(ops["grad_x"], ANISO), ops["grad"])
     assert np.array_equal(O.div(ops["div_v"], ANISO), ops["div"])
     for name, bct in (("gs_dir", O.BC_DIR), ("gs_neu", O.BC_NEU)):
@@ -73,6 +76,7 @@ def test_gpu_ops_match_golden(ctx, ops):
     assert rel(ctx.gauss_filter(ops["conv_x"], 2.0), ops["conv_iso"]) < 1e-13
     assert rel(ctx.gauss_filter(ops["conv_x"], 1.5, h=ANISO, pixel_approach=True),
                ops["conv_aniso_gpa"]) < 1e-13
+    assert rel(ctx.gauss_filter(ops["conv_x"], 2.0, h=ANISO, cyclic=True), ops["conv_cyclic"]) < 1e-13
     assert np.array_equal(ctx.grad(ops["grad_x"], ANISO), ops["grad"])
     assert np.array_equal(ctx.div(ops["div_v"], ANISO), ops["div"])
     for name, bct in (("gs_dir", 2), ("gs_neu", 1)):

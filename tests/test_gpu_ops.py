@@ -27,6 +27,17 @@ def test_gauss_filter(ctx, O, shape, h):
     assert rel(got32, want) < 2e-6
 
 
+@pytest.mark.parametrize("case", [((20, 22, 24), (1.0, 1.0, 1.0), 2.0), ((9, 14, 11), (0.8, 1.1, 1.3), 1.5),
+                                  ((7, 5, 30), (1.0, 1.0, 1.0), 3.0), ((40, 36, 33), (1.0, 1.0, 1.0), 3.0)])
+def test_gauss_filter_cyclic(ctx, O, case):
+    shape, h, sigma = case
+    x = np.random.default_rng(12).random(shape)
+    want = O.gauss_filter(x, sigma, h=h, cyclic=True)
+    assert rel(ctx.gauss_filter(x, sigma, h=h, cyclic=True), want) < 1e-13
+    got32 = ctx.gauss_filter(x.astype(np.float32), sigma, h=h, cyclic=True)
+    assert rel(got32, want) < 2e-6
+
+
 def test_gauss_filter_pixel_approach_and_radius(ctx, O):
     x = np.random.default_rng(11).random((16, 15, 14))
     for gpa in (False, True):

@@ -35,6 +35,8 @@ def _both(ctx, pkg, O, u0, phi0, dtype=np.float64, **kw):
     dict(bc=2, gs_rel_res_tol=1e-6, maxiter=20),
     dict(bc=2, init_variables=1), dict(bc=2, lamda1=1.0, lamda2=2.0),
     dict(bc=2, edge_detector_sigma=1.0), dict(bc=2, gaussian_pixel_approach=1),
+    dict(bc=2, conv_cyclic=1), dict(bc=1, conv_cyclic=1, edge_detector_sigma=1.0),
+    dict(bc=2, conv_cyclic=1, gs_rel_res_tol=1e-6),
 ])
 def test_apply_fp64_matches_checker(ctx, pkg, O, mode):
     u0, phi0 = _case(pkg)

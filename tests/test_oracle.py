@@ -33,6 +33,21 @@ def test_separable_conv_equals_reference_fft_and_direct(O, h, gpa):
     assert np.abs(a - direct).max() < 1e-14
 
 
+@pytest.mark.parametrize("case", [((20, 22, 24), (1.0, 1.0, 1.0), False, 2.0),
+                                  ((9, 14, 11), (0.8, 1.1, 1.3), True, 1.5),
+                                  ((7, 5, 30), (1.0, 1.0, 1.0), False, 3.0),
+                                  ((12, 10, 8), (1.0, 0.9, 1.2), False, 2.5)])
+def test_cyclic_conv_equals_reference(O, case):
+    # cyclic_fftw_convolution: periodic boundary, also on axes shorter than the kernel
+    _need_ref(O)
+    shape, h, gpa, sigma = case
+    x = np.random.default_rng(5).random(shape)
+    a = O.gauss_filter(x, sigma, h=h, pixel_approach=gpa, cyclic=True)
+    b = O.ref_gauss_filter(x, sigma, h=h, pixel_approach=gpa, cyclic=True)
+    assert np.abs(a - b).max() < 1e-14
+    assert not np.allclose(a, O.gauss_filter(x, sigma, h=h, pixel_approach=gpa))
+
+
 @pytest.mark.parametrize("shape", [(7, 9, 11), (3, 3, 3), (5, 4, 3)])
 @pytest.mark.parametrize("h", [(1.0, 1.0, 1.0), (0.8, 1.1, 1.3)])
 def test_grad_div_bit_exact_vs_reference(O, shape, h):
@@ -64,7 +79,8 @@ def test_change_range_matches_reference(O):
     assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("mode", ["lex-dir", "lex-neu", "default", "rb", "solve"])
+@pytest.mark.parametrize("mode", ["lex-dir", "lex-neu", "default", "rb", "solve", "cyclic",
+                                  "cyclic-neu-edge"])
 def test_full_loop_restatement_vs_reference(O, pkg, mode):
     _need_ref(O)
     shape = (20, 18, 16)
@@ -73,7 +89,9 @@ def test_full_loop_restatement_vs_reference(O, pkg, mode):
     kw = dict(sigma=2.0, lamda1=1.0, lamda2=1.0, lamda=0.5, maxiter=5, ls_steps=1, tol=0.0)
     kw.update({"lex-dir": dict(bc=O.BC_DIR), "lex-neu": dict(bc=O.BC_NEU), "default": {},
                "rb": dict(bc=O.BC_DIR, sweep=O.SWEEP_RB),
-               "solve": dict(bc=O.BC_DIR, gs_rel_res_tol=1e-6)}[mode])
+               "solve": dict(bc=O.BC_DIR, gs_rel_res_tol=1e-6),
+               "cyclic": dict(bc=O.BC_DIR, conv_cyclic=1),
+               "cyclic-neu-edge": dict(bc=O.BC_NEU, conv_cyclic=1, edge_detector_sigma=1.0)}[mode])
     p = O.default_params(**kw)
     a = O.rsfe_apply(u0, phi0, p)
     b = O.rsfe_apply(u0, phi0, p, use_reference=True)
