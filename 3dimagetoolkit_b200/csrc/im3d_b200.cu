@@ -263,7 +263,6 @@ int check_dims(im3d_ctx* ctx, int nx, int ny, int nz, double hx, double hy, doub
 }
 
 dim3 grid_vol(const Dims& d, dim3 blk) { return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, d.nx); }
-dim3 grid_pk(const Dims& d, dim3 blk) { return dim3((d.hz() + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, d.nx); }
 
 const dim3 kBlkVol(32, 8, 1);
 
@@ -532,12 +531,6 @@ int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c
 constexpr int kNI = 8;  // planes per thread of the scalar column-marching kernels
 constexpr int kNV = 2;  // planes per thread of the vectorised kernels (measured best on B200)
 const dim3 kBlkVec(32, 4, 1);
-
-dim3 grid_col_pk(const Dims& d, dim3 blk, int zmul = 1)
-{
-    return dim3((d.hz() + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y,
-                ((d.nx + kNI - 1) / kNI) * zmul);
-}
 
 // vector groups of 16 bytes along the packed rows
 template <typename T>

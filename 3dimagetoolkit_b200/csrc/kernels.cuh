@@ -831,84 +831,6 @@ __device__ __forceinline__ double gs_residual_fp64(const GsCoef<T>& c, const Dim
     return tx * c.ihx2d + ty * c.ihy2d + tz * c.ihz2d + b - diag * u;
 }
 
-// Red-black half sweep on the packed layout, one thread per packed column (m, j)
-// marching over NI planes of i. The other colour's value at (i, j, m) is the k
-// neighbour on one side of the point of plane i and the i neighbour of the points of
-// planes i-1 and i+1, so a three-deep register window along i serves six of the
-// eight neighbour reads; the other k neighbour is at m-1 (k even) or m+1 (k odd).
-// Interior points take a branch-free path; Neumann boundary points the generic one.
-template <typename T, int NI>
-__global__ void __launch_bounds__(256) rb_half_col_kernel(T* __restrict__ U,
-                                                          const T* __restrict__ B, Dims d,
-                                                          GsCoef<T> c, int color, int use_self,
-                                                          T omega)
-{
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i0 = blockIdx.z * NI;
-    const int hz = d.hz();
-    if (m >= hz || j >= d.ny) return;
-    const long long plane = (long long)d.ny * hz;
-    const long long npk = plane * d.nx;
-    T* own = U + (color ? npk : 0);
-    const T* oth = U + (color ? 0 : npk);
-    const T* bb = B + (color ? npk : 0);
-    const bool jint = j >= 1 && j <= d.ny - 2;
-    const long long q0 = ((long long)i0 * d.ny + j) * hz + m;
-    const bool relax = omega != T(1);
-    // all loads of the column first (fixed trip count, predicated), then the updates
-    T o[NI + 2];  // other colour at planes i0-1 .. i0+NI
-    T ys[NI], kn[NI], bv[NI], sf[NI];
-#pragma unroll
-    for (int t = 0; t < NI + 2; ++t) {
-        const int i = i0 - 1 + t;
-        o[t] = (i >= 0 && i < d.nx) ? oth[q0 + (long long)(t - 1) * plane] : T(0);
-    }
-#pragma unroll
-    for (int t = 0; t < NI; ++t) {
-        const int i = i0 + t;
-        const long long q = q0 + (long long)t * plane;
-        const int k = 2 * m + ((i + j + color) & 1);
-        const bool in = i >= 1 && i <= d.nx - 2 && jint && k >= 1 && k <= d.nz - 2;
-        ys[t] = in ? oth[q - hz] + oth[q + hz] : T(0);
-        kn[t] = in ? ((k & 1) ? oth[q + 1] : oth[q - 1]) : T(0);
-        bv[t] = in ? bb[q] : T(0);
-        sf[t] = (in && (use_self || relax)) ? own[q] : T(0);
-    }
-#pragma unroll
-    for (int t = 0; t < NI; ++t) {
-        const int i = i0 + t;
-        if (i >= d.nx) break;
-        const long long q = q0 + (long long)t * plane;
-        const int k = 2 * m + ((i + j + color) & 1);
-        if (k >= d.nz) continue;
-        if (jint && i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2) {
-            const T sz = o[t + 1] + kn[t];
-            const T sy = ys[t];
-            const T sx = o[t] + o[t + 2];
-            const T b = bv[t];
-            const T self = sf[t];
-            T v;
-            if (std::is_same<T, double>::value) {
-                double acc = sx / (c.hx * c.hx) + sy / (c.hy * c.hy) + sz / (c.hz * c.hz) + b;
-                if (use_self) acc = acc + self / c.dt;
-                v = T(acc * (double)c.htilde[7]);
-            } else {
-                T acc = fma(sx, c.ihx2, fma(sy, c.ihy2, fma(sz, c.ihz2, b)));
-                if (use_self) acc = fma(self, c.idt, acc);
-                v = acc * c.htilde[7];
-            }
-            if (relax) v = self + omega * (v - self);
-            own[q] = v;
-        } else if (c.neu) {
-            auto rd = [&](int oi, int oj, int ok) { return oth[d.pidx(i + oi, j + oj, k + ok)]; };
-            const T self = own[q];
-            T v = gs_value<T>(c, d, i, j, k, bb[q], self, use_self != 0, rd);
-            if (relax) v = self + omega * (v - self);
-            own[q] = v;
-        }
-    }
-}
 
 // Vectorised red-black half sweep: one thread per group of W = 16/sizeof(T)
 // consecutive packed points (m0 .. m0+W-1) of row j, marching over NI planes of i.
@@ -1135,75 +1057,6 @@ __global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restric
     else block_sum_store(acc, part);
 }
 
-// FP64 residual of (1/dt - Lap) u = b_eff on the packed layout, same column walk;
-// blockIdx.z covers (plane block, colour). Accumulates sum r^2 and, when asked,
-// sum b_eff^2 over the unknowns.
-template <typename T, int NI>
-__global__ void __launch_bounds__(256) rb_residual_col_kernel(const T* __restrict__ U,
-                                                              const T* __restrict__ B, Dims d,
-                                                              GsCoef<T> c, double* part,
-                                                              int want_beff)
-{
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int color = blockIdx.z & 1;
-    const int i0 = (blockIdx.z >> 1) * NI;
-    const int hz = d.hz();
-    double acc = 0, accb = 0;
-    if (m < hz && j < d.ny) {
-        const long long plane = (long long)d.ny * hz;
-        const long long npk = plane * d.nx;
-        const T* own = U + (color ? npk : 0);
-        const T* oth = U + (color ? 0 : npk);
-        const T* bb = B + (color ? npk : 0);
-        const bool jint = j >= 1 && j <= d.ny - 2;
-        const int lo = c.neu ? 0 : 1;
-        const long long q0 = ((long long)i0 * d.ny + j) * hz + m;
-        double o[NI + 2];
-#pragma unroll
-        for (int t = 0; t < NI + 2; ++t) {
-            const int i = i0 - 1 + t;
-            o[t] = (i >= 0 && i < d.nx) ? (double)oth[q0 + (long long)(t - 1) * plane] : 0.0;
-        }
-        double ys[NI], kn[NI], bv[NI], uv[NI];
-#pragma unroll
-        for (int t = 0; t < NI; ++t) {
-            const int i = i0 + t;
-            const long long q = q0 + (long long)t * plane;
-            const int k = 2 * m + ((i + j + color) & 1);
-            const bool in = i >= 1 && i <= d.nx - 2 && jint && k >= 1 && k <= d.nz - 2;
-            const bool any = i < d.nx && k < d.nz;
-            ys[t] = in ? (double)oth[q - hz] + (double)oth[q + hz] : 0.0;
-            kn[t] = in ? ((k & 1) ? (double)oth[q + 1] : (double)oth[q - 1]) : 0.0;
-            bv[t] = any ? (double)bb[q] : 0.0;
-            uv[t] = any ? (double)own[q] : 0.0;
-        }
-#pragma unroll
-        for (int t = 0; t < NI; ++t) {
-            const int i = i0 + t;
-            if (i >= d.nx) break;
-            const long long q = q0 + (long long)t * plane;
-            const int k = 2 * m + ((i + j + color) & 1);
-            if (k >= d.nz) continue;
-            if (jint && i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2) {
-                const double r = (o[t] + o[t + 2]) * c.ihx2d + ys[t] * c.ihy2d +
-                                 (o[t + 1] + kn[t]) * c.ihz2d + bv[t] - c.diagd * uv[t];
-                acc += r * r;
-                accb += bv[t] * bv[t];
-            } else if (i >= lo && j >= lo && k >= lo && i < d.nx - lo && j < d.ny - lo &&
-                       k < d.nz - lo) {
-                auto rd = [&](int oi, int oj, int ok) {
-                    return (double)oth[d.pidx(i + oi, j + oj, k + ok)];
-                };
-                const double r = gs_residual_fp64<T>(c, d, i, j, k, bv[t], uv[t], rd);
-                acc += r * r;
-                accb += bv[t] * bv[t];
-            }
-        }
-    }
-    if (want_beff) block_sum2_store(acc, accb, part);
-    else block_sum_store(acc, part);
-}
 
 // cut_phi (rsfe_splitbregman_imp.hxx:320-339) and the tolerance sums of :1832:
 // phi holds phiold on entry and the clamped solve result on exit (natural layout);
@@ -1571,7 +1424,6 @@ __global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict_
     const int kb = g * W;
     double s_d = 0, s_o = 0;
     if (kb < d.nz && j < d.ny) {
-        const long long plane = (long long)d.ny * d.nz;
         const long long pplane = (long long)d.ny * d.hz();
         const long long npk = pplane * d.nx;
 #pragma unroll
@@ -1821,15 +1673,8 @@ __global__ void make_beff_kernel(const T* __restrict__ b, T* __restrict__ U, T* 
     if (part) block_sum_store(acc, part);
 }
 
-// ------------------------------------------------------------------ utilities
-template <typename T>
-__global__ void fill_kernel(T* p, long long n, T v)
-{
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-         q += (long long)gridDim.x * blockDim.x)
-        p[q] = v;
-}
 
+// ------------------------------------------------------------------ utilities
 // min / max of a volume as order-preserving unsigned keys (umax[0] = max, umax[1] = max of -x)
 __device__ __forceinline__ unsigned long long order_key(double x)
 {
