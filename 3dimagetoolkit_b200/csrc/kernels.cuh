@@ -1589,20 +1589,30 @@ __global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T
             const VV ym = *reinterpret_cast<const VV*>(f1 + p - sy);
             const VV yp = *reinterpret_cast<const VV*>(f1 + p + sy);
             const VV zc = *reinterpret_cast<const VV*>(f2 + p);
-            const T km = kb >= 1 ? f2[p - 1] : T(0);
-            const T kp = kb + W < d.nz ? f2[p + W] : T(0);
+            // f2 at k = kb-1 .. kb+W: zz[c + 1] = f2[kb + c]
+            T zz[W + 2];
+            zz[0] = kb >= 1 ? f2[p - 1] : T(0);
+#pragma unroll
+            for (int c = 0; c < W; ++c) zz[c + 1] = VT::get(zc, c);
+            zz[W + 1] = kb + W < d.nz ? f2[p + W] : T(0);
+            // i and j inside: div_point's x and y terms are central, and its z term is
+            // central or, on the faces k = 0 and k = nz-1, grad_term's one-sided
+            // difference; evaluated here with the same operations, without a branch
 #pragma unroll
             for (int cc = 0; cc < W; ++cc) {
                 const int k = kb + cc;
-                if (k >= 1 && k <= d.nz - 2) {
-                    const T tx = (VT::get(x[t + 2], cc) - VT::get(x[t], cc)) / two_hx;
-                    const T ty = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
-                    const T zp = cc + 1 < W ? VT::get(zc, cc + 1) : kp;
-                    const T zm = cc >= 1 ? VT::get(zc, cc - 1) : km;
-                    VT::set(o, cc, tx + ty + (zp - zm) / two_hz);
-                } else {
-                    VT::set(o, cc, div_point(f0, f1, f2, d, i, j, k, hx, hy, hz));
+                const T tx = (VT::get(x[t + 2], cc) - VT::get(x[t], cc)) / two_hx;
+                const T ty = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
+                T tz = (zz[cc + 2] - zz[cc]) / two_hz;
+                if (cc == 0) {
+                    const T lo = (T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3]) / two_hz;
+                    tz = k == 0 ? lo : tz;
                 }
+                if (cc == W - 1) {
+                    const T hi = (T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1]) / two_hz;
+                    tz = k == d.nz - 1 ? hi : tz;
+                }
+                VT::set(o, cc, tx + ty + tz);
             }
         } else {
 #pragma unroll
