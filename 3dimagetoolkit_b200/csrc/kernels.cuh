@@ -1465,8 +1465,8 @@ __global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict_
     block_sum2_store(s_d, s_o, part);
 }
 
-// Split-Bregman update (see bregman_kernel), vectorised along k; points on a face of
-// the volume take the scalar one-sided stencils.
+// Split-Bregman update (see bregman_kernel), vectorised along k; rows on an i or j face
+// of the volume take the scalar one-sided stencils.
 template <typename T, int NI>
 __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ phi,
                                                           T* __restrict__ b3, T* __restrict__ dmb,
@@ -1505,8 +1505,12 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
             ym = *reinterpret_cast<const VV*>(phi + p - sy);
             yp = *reinterpret_cast<const VV*>(phi + p + sy);
         }
-        const T km = kb >= 1 ? phi[p - 1] : T(0);
-        const T kp = kb + W < d.nz ? phi[p + W] : T(0);
+        // phi at k = kb-1 .. kb+W of this row: zz[c + 1] = phi[kb + c]
+        T zz[W + 2];
+        zz[0] = kb >= 1 ? phi[p - 1] : T(0);
+#pragma unroll
+        for (int c = 0; c < W; ++c) zz[c + 1] = VT::get(f[t + 1], c);
+        zz[W + 1] = kb + W < d.nz ? phi[p + W] : T(0);
         const VV gg = *reinterpret_cast<const VV*>(g3 + p);
         VV bo[3], dn[3];
 #pragma unroll
@@ -1515,12 +1519,22 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
         for (int cc = 0; cc < W; ++cc) {
             const int k = kb + cc;
             T gr[3];
-            if (rowint && k >= 1 && k <= d.nz - 2) {
+            if (rowint) {
+                // i and j inside: central x and y terms; the z term is central or, on
+                // the faces k = 0 and k = nz-1, grad_term's one-sided difference,
+                // evaluated with the same operations without a branch
                 gr[0] = (VT::get(f[t + 2], cc) - VT::get(f[t], cc)) / two_hx;
                 gr[1] = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
-                const T fkp = cc + 1 < W ? VT::get(f[t + 1], cc + 1) : kp;
-                const T fkm = cc >= 1 ? VT::get(f[t + 1], cc - 1) : km;
-                gr[2] = (fkp - fkm) / two_hz;
+                T tz = (zz[cc + 2] - zz[cc]) / two_hz;
+                if (cc == 0) {
+                    const T lo = (T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3]) / two_hz;
+                    tz = k == 0 ? lo : tz;
+                }
+                if (cc == W - 1) {
+                    const T hi = (T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1]) / two_hz;
+                    tz = k == d.nz - 1 ? hi : tz;
+                }
+                gr[2] = tz;
             } else {
                 const long long pc = p + cc;
                 gr[0] = grad_term(phi, pc, plane, i, d.nx, hx);
@@ -1548,8 +1562,8 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
     }
 }
 
-// im3d::div vectorised along k (see div_point); points on a face of the volume take
-// the scalar rule with the reference's quirks.
+// im3d::div vectorised along k (see div_point); rows on an i or j face of the volume
+// take the scalar rule with the reference's quirks.
 template <typename T, int NI>
 __global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T* __restrict__ out,
                                                       Dims d, double hx, double hy, double hz)
