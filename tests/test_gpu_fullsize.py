@@ -1,0 +1,55 @@
+"""GPU: the benchmark workloads at full size, through properties that do not need the
+CPU checker (which would take hours at these sizes):
+
+- the FP32 path against the FP64 path on the same seed and solve tolerance. After 10
+  outer iterations at 256^3 the fields meet the per-field bars of the workload (u, f1,
+  f2 relative L2 <= 1e-5); over a full run the FP32 rounding of each outer iteration
+  (~2e-7) accumulates, since the outer iteration does not damp earlier errors, so the
+  full runs are held to the segmentation bars (sign(phi - 0.5) agreement >= 99.9 %, Dice >=
+  0.999) and to bounds on the field drift about three times what was measured on B200
+  (256^3, 100 it.: u 9.2e-5, f1 2.0e-5, f2 2.9e-5; 512x512x320, 200 it.: u 1.8e-3, f1
+  5.0e-4, f2 4.3e-4, Dice 0.99967; an FP64 run at the same tolerance is itself 1.9e-5
+  from a fully converged one at 256^3); the FP64 path is checked against the checker at
+  smaller sizes;
+- every Poisson solve reached the relative residual it was asked for;
+- a second run gives bit-identical results (deterministic reductions and sweeps)."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, bc=2, tol=0.0,
+              gs_rel_res_tol=1e-6, gs_max_sweeps=1000)
+# workload, outer iterations, bounds on the relative L2 of (u, f1, f2)
+CASES = [("c2", dict(maxiter=10), (1e-5, 1e-5, 1e-5)),
+         ("c2", dict(maxiter=100), (3e-4, 1e-4, 1e-4)),
+         ("c3", dict(maxiter=200, sigma=4.0), (5e-3, 1.5e-3, 1.5e-3))]
+
+
+@pytest.mark.parametrize("name, kw, bounds", CASES)
+def test_fp32_against_fp64(ctx, pkg, name, kw, bounds):
+    u0, phi0 = pkg.synth.config_volume(name, seed=0)
+    kw = {**PARAMS, **kw}
+    got = ctx.rsfe_apply(u0.astype(np.float32), phi0.astype(np.float32), pkg.default_params(**kw),
+                         want_u=True, want_f=True)
+    ref = ctx.rsfe_apply(u0, phi0, pkg.default_params(**kw), want_u=True, want_f=True)
+    for r in (got, ref):
+        assert r["stats"]["iterations"] == kw["maxiter"]
+        assert r["stats"]["not_converged"] == 0
+        assert r["stats"]["last_rel_res"] <= 1e-6
+    for key, bound in zip(("u", "f1", "f2"), bounds):
+        assert rel(got[key], ref[key]) <= bound, key
+    agree = np.mean((got["phi"] > 0.5) == (ref["phi"] > 0.5))
+    assert agree >= 0.999
+    assert pkg.synth.dice(got["phi"], ref["phi"]) >= 0.999
+
+
+def test_fp32_runs_are_bit_identical(ctx, pkg):
+    u0, phi0 = pkg.synth.config_volume("c2", seed=1, dtype=np.float32)
+    p = pkg.default_params(**{**PARAMS, "maxiter": 20})
+    a = ctx.rsfe_apply(u0, phi0, p, want_u=True)
+    b = ctx.rsfe_apply(u0, phi0, p, want_u=True)
+    assert np.array_equal(a["phi"], b["phi"]) and np.array_equal(a["u"], b["u"])
+    assert a["stats"]["total_sweeps"] == b["stats"]["total_sweeps"]
