@@ -38,7 +38,7 @@ struct im3d_ctx {
     std::unordered_map<std::string, DevBuf> bufs;
     Ctrl* ctrl_d = nullptr;
     Ctrl* ctrl_h = nullptr;  // pinned
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [3]: tolerance copy done
     // per-stage device timing (im3d_ctx_set_profiling): events recorded on the
     // launching stream around each launch, resolved at the next synchronisation
     bool prof = false;
@@ -1274,6 +1274,12 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                 IM3D_TRY(finalize(ctx, part, grid, 2, SUM_DPHI2));
             }
         }
+        // the tolerance sums are final here: copy them out now and wait only for that
+        // copy after the Bregman update is queued, so that the next iteration's kernels
+        // queue behind work that is still running
+        IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->ctrl_h, ctx->ctrl_d, sizeof(Ctrl), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+        IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
         if (init_variables) {
             IM3D_CUDA(ctx, cudaMemsetAsync(divdb, 0, n * sizeof(T), ctx->stream));
             IM3D_CUDA(ctx, cudaMemsetAsync(b3, 0, 3 * n * sizeof(T), ctx->stream));
@@ -1297,7 +1303,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             prof_end(ctx, pf2);
             IM3D_TRY(check_launch(ctx, "div"));
         }
-        IM3D_TRY(read_ctrl(ctx));
+        if (cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) IM3D_TRY(sync(ctx));
         tollerance = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_DPHI2]) /
                      std::sqrt(hhh * ctx->ctrl_h->sum[SUM_PHIOLD2]);
         if (lex) std::swap(phi, other);
@@ -1728,7 +1734,8 @@ int im3d_ctx_create(int device, im3d_ctx** out)
         delete ctx;
         return IM3D_ERR_CUDA;
     }
-    for (auto& e : ctx->ev) cudaEventCreate(&e);
+    for (int q = 0; q < 3; ++q) cudaEventCreate(&ctx->ev[q]);
+    cudaEventCreateWithFlags(&ctx->ev[3], cudaEventDisableTiming);
     ctx->stream = ctx->own_stream;
     // L2 pinning of the Gauss-Seidel state is opt-in (IM3D_L2_PERSIST=1): on B200 the
     // set-aside speeds the half-sweep up (26.9 -> 22.9 us at 256^3) but slows the
