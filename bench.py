@@ -61,9 +61,9 @@ ALGO_BYTES_PER_VOXEL = {
 }
 
 WORKLOADS = {
-    # the headline
+    # the 256^3 workload (the headline)
     "c2": dict(shape=(256, 256, 256), maxiter=100, sigma=3.0),
-    # CT-shaped single volume
+    # the 512x512x320 CT-shaped single volume
     "c3": dict(shape=(512, 512, 320), maxiter=200, sigma=4.0),
 }
 

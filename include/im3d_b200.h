@@ -257,7 +257,7 @@ int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, 
                                  int nz, const double* init, int i, int j, int k, double threshold,
                                  int full_connected, int binary_output, int* passes);
 
-/* A batch of independent volumes (BASELINE's uneven-volume workload). No counterpart
+/* A batch of independent volumes of uneven sizes. No counterpart
  * in the reference, which segments one image per apply(). Each descriptor holds the
  * caller's buffers (host or device, T = float for _f32, double for _f64), the size
  * and the spacing. */
