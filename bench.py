@@ -140,6 +140,33 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------- GPU arm
+def unet_flop_estimate(shape):
+    """FLOPs (2 per multiply-add) of one inference of the learned warm start's network:
+    3 levels of two 3x3x3 convolutions (16, 32, 64 channels; 4 input fields: rhs,
+    previous u, div(d - b), phi), 2x down- and up-sampling, skip connections
+    concatenated, a 1x1x1 output convolution."""
+    n1 = shape[0] * shape[1] * shape[2]
+    n2, n3 = n1 / 8.0, n1 / 64.0
+    k = 27
+    macs = n1 * k * (4 * 16 + 16 * 16)            # level 1, encoder
+    macs += n2 * k * (16 * 32 + 32 * 32)          # level 2, encoder
+    macs += n3 * k * (32 * 64 + 64 * 64)          # level 3
+    macs += n3 * 8 * 64 * 32 + n2 * 8 * 32 * 16   # 2x2x2 transposed convolutions
+    macs += n2 * k * (64 * 32 + 32 * 32)          # level 2, decoder (skip concatenated)
+    macs += n1 * k * (32 * 16 + 16 * 16)          # level 1, decoder
+    macs += n1 * 16                               # output
+    return 2.0 * macs
+
+
+def bf16_peak_tflops():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"])
+    return 1590.0
+
+
 def half_sweep_us(ctx, shape, dev, stream):
     """Device time of one red-black half-sweep inside a Poisson solve, in us."""
     import torch
@@ -331,6 +358,30 @@ def run_gpu(args):
                       "algo_gbs": (round(ALGO_BYTES_PER_VOXEL[k] * n * v[1] / (v[0] * 1e-3) / 1e9, 1)
                                    if k in ALGO_BYTES_PER_VOXEL and v[0] > 0 else None)}
                   for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+        # learned Poisson warm start (3-level 3x3x3 U-Net, 16/32/64 channels, 4 inputs):
+        # an upper bound on its time-to-residual gain from measured numbers -- the plain
+        # solve's device time per outer iteration against the network's FLOPs at the
+        # measured dense bf16 peak, i.e. a perfect prediction (no sweeps after it) and a
+        # network at 100 % of that peak. Not a measurement of a built network.
+        solve_ms = 0.0
+        for k, (m, c) in prof.items():
+            if k == "rb_half":
+                solve_ms += (sweep_us * 1e-3 * c) if sweep_us else m
+            elif k in ("rb_residual", "rb_pair"):
+                solve_ms += m
+        solve_ms_iter = solve_ms / max(kw["maxiter"], 1)
+        unet_flop = unet_flop_estimate(shape)
+        bf16 = bf16_peak_tflops()
+        unet_ms = unet_flop / (bf16 * 1e12) * 1e3 if bf16 else None
+        learned = {
+            "plain_solve_ms_per_outer_iteration": solve_ms_iter,
+            "unet_gflop_per_inference": unet_flop / 1e9,
+            "bf16_peak_tflops": bf16,
+            "unet_ms_at_peak": unet_ms,
+            "speedup_upper_bound": (solve_ms_iter / unet_ms) if unet_ms else None,
+            "target": 2.0,
+            "note": "bound from measured figures, no network is built",
+        }
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt_ms / args.steps, "higher_is_better": True,
@@ -346,6 +397,7 @@ def run_gpu(args):
             "e2e": {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 4,
                     "d2h_bytes_per_step": n * 4, "ms_per_step": e_ms / args.steps},
             "roofline": roofline, "stages_ms_per_step": stages, "gpu_launches": launches,
+            "learned_warm_start_bound": learned,
             "clocks": clocks,
         }
         if args.workload != "c2":
