@@ -63,6 +63,7 @@ struct im3d_ctx {
     bool tb_enabled = false;
     int pair_resident[2] = {0, 0};  // resident rb_pair_kernel CTAs (24- and 22-row tiles)
     int num_sms = 148;
+    int ifit_chunks = 0;  // i chunks of the marching fit stage (0: cost model)
     long long residual_checks = 0;  // rb_check calls, for the statistics
 };
 
@@ -300,6 +301,7 @@ template <typename T>
 struct Taps {
     const T* w[3];
     int nh[3];
+    T host[3][NH_MAX];  // the same taps on the host (kernels that take them by value)
 };
 
 template <typename T>
@@ -330,6 +332,7 @@ int upload_taps(im3d_ctx* ctx, const char* slot, double sigma, double radius, do
     for (int a = 0; a < 3; ++a) {
         out->w[a] = d + a * NH_MAX;
         out->nh[a] = nh[a];
+        for (int t = 0; t < NH_MAX; ++t) out->host[a][t] = host[a * NH_MAX + t];
     }
     return IM3D_OK;
 }
@@ -436,10 +439,54 @@ int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T*
     return check_launch(ctx, "conv_i_fit");
 }
 
+// Marching i-stage (FP32): one (j, k) column per thread, chunks of i per blockIdx.z.
+// The kernel is issue-bound, so the chunk count minimises the planes one SM streams:
+// ceil(blocks / SMs) x (chunk + 4S), where each chunk re-streams 4S halo planes
+// (measured at 256^3: 1, 2, 3, 4 chunks take 152, 144, 160, 164 us; this picks 2).
+// IM3D_IFIT_CHUNKS overrides it.
+template <int S>
+int pass_i_fit_march(im3d_ctx* ctx, const Vec<float, 4>* in, Vec<float, 2>* out, float* f1,
+                     float* f2, const Dims& d, const float* hw, float l1, float l2)
+{
+    // 4 blocks of 128 threads per SM for 19 taps (126 registers, no spills); 2 for 25
+    // taps (3 would spill)
+    constexpr int JB = 4, D = 16, U = 4, MINB = S <= 9 ? 4 : 2;
+    auto kern = conv_i_fit_march_kernel<S, JB, D, U, MINB>;
+    const long long cols = (long long)((d.nz + 31) / 32) * ((d.ny + JB - 1) / JB);
+    int chunks = ctx->ifit_chunks;
+    if (chunks <= 0) {
+        long long best = 0;
+        for (int c = 1; c <= 8 && c <= d.nx; ++c) {
+            const int chunk = (d.nx + c - 1) / c;
+            const long long per_sm = (cols * c + ctx->num_sms - 1) / ctx->num_sms;
+            const long long cost = per_sm * (chunk + 4 * S);
+            if (c == 1 || cost < best) {
+                best = cost;
+                chunks = c;
+            }
+        }
+    }
+    chunks = std::min(chunks, d.nx);
+    const int chunk = (d.nx + chunks - 1) / chunks;
+    dim3 grid((d.nz + 31) / 32, (d.ny + JB - 1) / JB, (d.nx + chunk - 1) / chunk);
+    TapPairs<S> tp;
+    for (int t = 0; t <= S; ++t) tp.w[t] = make_float2(hw[t], hw[t]);
+    const int pf = prof_begin(ctx, "conv_i_fit");
+    kern<<<grid, dim3(32, JB), 0, ctx->stream>>>(reinterpret_cast<const float4*>(in),
+                                                 reinterpret_cast<float2*>(out), f1, f2, d, tp,
+                                                 l1, l2, chunk);
+    prof_end(ctx, pf);
+    return check_launch(ctx, "conv_i_fit");
+}
+
 template <typename T>
 int pass_i_fit(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T* f2, const Dims& d,
-               const T* w, int nh, T l1, T l2)
+               const T* w, const T* hw, int nh, T l1, T l2)
 {
+    if constexpr (sizeof(T) == 4) {
+        if (nh == 19) return pass_i_fit_march<9>(ctx, in, out, f1, f2, d, hw, l1, l2);
+        if (nh == 25) return pass_i_fit_march<12>(ctx, in, out, f1, f2, d, hw, l1, l2);
+    }
     if (nh == 19) return pass_i_fit_win<T, 9>(ctx, in, out, f1, f2, d, w, l1, l2);
     if (nh == 25) return pass_i_fit_win<T, 12>(ctx, in, out, f1, f2, d, w, l1, l2);
     constexpr int TA = TileA<T>::v;
@@ -1150,7 +1197,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                                d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
         IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1],
                                   "conv_s_j4")));
-        IM3D_TRY(pass_i_fit<T>(ctx, W2, P1, f1_d, f2_d, d, tp.w[0], tp.nh[0], (T)p->lamda1,
+        IM3D_TRY(pass_i_fit<T>(ctx, W2, P1, f1_d, f2_d, d, tp.w[0], tp.host[0], tp.nh[0], (T)p->lamda1,
                                (T)p->lamda2));
         IM3D_TRY((pass_s<T, 2, 1>(ctx, LdVec<T, 2>{P1, d}, StVec<T, 2>{P2, d}, d, tp.w[1], tp.nh[1],
                                   "conv_s_j2")));
@@ -1747,6 +1794,8 @@ int im3d_ctx_create(int device, im3d_ctx** out)
                            ? (size_t)prop.persistingL2CacheMaxSize : 0;
     ctx->window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
     ctx->num_sms = prop.multiProcessorCount;
+    const char* ch = std::getenv("IM3D_IFIT_CHUNKS");
+    ctx->ifit_chunks = ch ? std::atoi(ch) : 0;
     *out = ctx;
     return IM3D_OK;
 }

@@ -61,10 +61,22 @@ struct LdVec {
     }
 };
 
+// A storer's pre() issues the reads that its store of cells k0 .. k0+cnt-1 of one row
+// needs, early in a pass, and put4() stores those cells; operator() stores one cell.
 template <typename T, int N>
 struct StVec {
     Vec<T, N>* p;
     Dims d;
+    struct Pre {};
+    __device__ __forceinline__ Pre pre(int, int, int, int) const { return Pre{}; }
+    __device__ __forceinline__ void put4(const Pre&, int i, int j, int k0, const Vec<T, N> (&v)[4],
+                                         int cnt) const
+    {
+        const long long q = d.idx(i, j, k0);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (r < cnt) p[q + r] = v[r];
+    }
     __device__ __forceinline__ void operator()(int i, int j, int k, const Vec<T, N>& v) const
     {
         p[d.idx(i, j, k)] = v;
@@ -103,11 +115,56 @@ template <typename T>
 struct StScalar {
     T* p;
     Dims d;
+    struct Pre {};
+    __device__ __forceinline__ Pre pre(int, int, int, int) const { return Pre{}; }
+    __device__ __forceinline__ void put4(const Pre&, int i, int j, int k0, const Vec<T, 1> (&v)[4],
+                                         int cnt) const
+    {
+        const long long q = d.idx(i, j, k0);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (r < cnt) p[q + r] = v[r].v[0];
+    }
     __device__ __forceinline__ void operator()(int i, int j, int k, const Vec<T, 1>& v) const
     {
         p[d.idx(i, j, k)] = v.v[0];
     }
 };
+
+// four consecutive values from p (16-byte vector reads when they are aligned), zero
+// past cnt
+template <typename T>
+__device__ __forceinline__ void ld4(const T* __restrict__ p, int cnt, T (&o)[4])
+{
+    if (cnt == 4 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+            o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+        } else {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+            const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+            o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) o[r] = r < cnt ? ld_g(p + r) : T(0);
+    }
+}
+
+// two values to p and p+1: one vector store when aligned
+template <typename T>
+__device__ __forceinline__ void st2(T* p, T a, T b)
+{
+    if ((reinterpret_cast<uintptr_t>(p) & (2 * sizeof(T) - 1)) == 0) {
+        Vec<T, 2> v;
+        v.v[0] = a;
+        v.v[1] = b;
+        *reinterpret_cast<Vec<T, 2>*>(p) = v;
+    } else {
+        p[0] = a;
+        p[1] = b;
+    }
+}
 
 // Stage-1 input: (H u0, H, Hb u0, Hb) from phi and u0.
 template <typename T>
@@ -156,6 +213,85 @@ struct StRhs {
     Dims d;
     T l12, lamda, inv_dt, bc;
     int mode, dirichlet;
+    struct Pre {
+        T u[4], kn[4], dv[4], ph[4];
+    };
+    __device__ __forceinline__ Pre pre(int i, int j, int k0, int cnt) const
+    {
+        Pre w;
+        const long long q = d.idx(i, j, k0);
+        ld4(u0 + q, cnt, w.u);
+        if (kones) ld4(kones + q, cnt, w.kn);
+        ld4(divdb + q, cnt, w.dv);
+        if (mode != 0) ld4(phi + q, cnt, w.ph);
+        return w;
+    }
+    // the forcing term of one cell, operations as in operator()
+    __device__ __forceinline__ T force(const Pre& w, int r, const Vec<T, 2>& v) const
+    {
+        const T u = w.u[r];
+        T f = v.v[0];
+        f *= u;
+        f *= T(2);
+        if (kones) {
+            T a = l12;
+            a *= u;
+            a *= u;
+            a *= w.kn[r];
+            f -= a;
+        }
+        f -= v.v[1];
+        f /= lamda;
+        f -= w.dv[r];
+        return f;
+    }
+    // k0 is even: cells k0, k0+2 have the colour of k0 and packed slots k0/2, k0/2+1,
+    // cells k0+1, k0+3 the other colour and the same two slots
+    __device__ __forceinline__ void put4(const Pre& w, int i, int j, int k0, const Vec<T, 2> (&v)[4],
+                                         int cnt) const
+    {
+        T f[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) f[r] = force(w, r, v[r]);
+        if (mode == 0) {
+            T* o = out + d.idx(i, j, k0);
+            if (cnt == 4) {
+                st2(o, f[0], f[1]);
+                st2(o + 2, f[2], f[3]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    if (r < cnt) o[r] = f[r];
+            }
+            return;
+        }
+        const bool face_ij = i == 0 || j == 0 || i == d.nx - 1 || j == d.ny - 1;
+        T ph[4], val[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            ph[r] = w.ph[r];
+            if (dirichlet && (face_ij || k0 + r == 0 || k0 + r == d.nz - 1)) ph[r] = bc;
+            val[r] = mode == 2 ? f[r] + ph[r] * inv_dt : f[r];
+        }
+        const int c0 = (i + j + k0) & 1;
+        const long long base = d.pidx(i, j, k0);
+        const long long o0 = base + (c0 ? d.npk() : 0), o1 = base + (c0 ? 0 : d.npk());
+        if (cnt == 4) {
+            st2(upk + o0, ph[0], ph[2]);
+            st2(upk + o1, ph[1], ph[3]);
+            st2(out + o0, val[0], val[2]);
+            st2(out + o1, val[1], val[3]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (r < cnt) {
+                    const long long o = ((r & 1) ? o1 : o0) + (r >> 1);
+                    upk[o] = ph[r];
+                    out[o] = val[r];
+                }
+            }
+        }
+    }
     __device__ __forceinline__ void operator()(int i, int j, int k, const Vec<T, 2>& v) const
     {
         const long long q = d.idx(i, j, k);
@@ -187,6 +323,27 @@ struct StRhs {
         out[pq] = mode == 2 ? r + ph * inv_dt : r;
     }
 };
+
+// ------------------------------------------------------------------- cp.async
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+// 16 bytes, or 16 zero bytes when !valid (nothing is read from gmem then)
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // ------------------------------------------------------- separable convolution
 // out = sum_t w[t] x[p + t - S], symmetric taps (w[t] == w[nh-1-t]), zero outside.
@@ -315,6 +472,8 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     const int i = live ? (int)(row / d.ny) : 0;
     const int j = live ? (int)(row % d.ny) : 0;
     const int k0 = blockIdx.y * TK;
+    const int kk = k0 + threadIdx.x * R;  // this thread's first output cell (even)
+    typename St::Pre pre{};
     {
         constexpr int NL = (W + TKT - 1) / TKT;
         // all reads first, then the loader's arithmetic (the Heaviside for stage 1)
@@ -327,6 +486,8 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
             ok[u] = s < W && live && d.halo(k0 - SP + s, d.nz, k);
             if (ok[u]) rw[u] = ld.raw(i, j, k);
         }
+        // the storer's own reads (the forcing term's fields) go out with them
+        if (kk < d.nz && live) pre = st.pre(i, j, kk, min(R, d.nz - kk));
         Vec<T, N> v[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) v[u] = ok[u] ? ld.cook(rw[u]) : vzero<T, N>();
@@ -342,7 +503,6 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     T w[S + 1];
     load_taps<T, S>(taps, w);
     __syncthreads();
-    const int kk = k0 + threadIdx.x * R;
     const bool act = live && kk < d.nz;
     T res[N][R];
     if (act) {
@@ -370,15 +530,13 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
         }
     }
     if (!act) return;
+    Vec<T, N> vo[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        if (kk + r < d.nz) {
-            Vec<T, N> v;
 #pragma unroll
-            for (int q = 0; q < N; ++q) v.v[q] = res[q][r];
-            st(i, j, kk + r, v);
-        }
+        for (int q = 0; q < N; ++q) vo[r].v[q] = res[q][r];
     }
+    st.put4(pre, i, j, kk, vo, min(R, d.nz - kk));
 }
 
 // Along j (AXIS 1) or i (AXIS 0). Block TW x TY; each thread R consecutive outputs
@@ -538,6 +696,143 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>*
             out[d.idx(i, j, k)] = v;
         }
     }
+}
+
+// One step of a running convolution along a march axis, on float pairs with the
+// packed f32x2 pipes. acc[u] holds the partial sum of row p - S + u, where p is the
+// plane being added: acc[u] <- acc[u+1] + w[u] x for u = 0 .. 2S-1 (w symmetric,
+// w[u] = w[2S-u]) and acc[2S] <- w[0] x. After the step acc[0] is complete: its row
+// has received w[t] x[row - S + t] for t = 0 .. 2S, in plane order. Every update
+// reads a slot before the one it writes, so the window shifts with no moves and the
+// 2S+1 updates of a step are independent.
+template <int S>
+__device__ __forceinline__ void shift_conv2(float2 (&acc)[2 * S + 1], const float2 (&w)[S + 1], float2 x)
+{
+#pragma unroll
+    for (int u = 0; u < 2 * S; ++u) acc[u] = __ffma2_rn(w[u <= S ? u : 2 * S - u], x, acc[u + 1]);
+    acc[2 * S] = __fmul2_rn(w[0], x);
+}
+
+// cp.async.wait_group with a count known only after unrolling (0 .. 15)
+__device__ __forceinline__ void cp_async_wait_n(int n)
+{
+    switch (n) {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    case 3: cp_async_wait<3>(); break;
+    case 4: cp_async_wait<4>(); break;
+    case 5: cp_async_wait<5>(); break;
+    case 6: cp_async_wait<6>(); break;
+    case 7: cp_async_wait<7>(); break;
+    case 8: cp_async_wait<8>(); break;
+    case 9: cp_async_wait<9>(); break;
+    case 10: cp_async_wait<10>(); break;
+    case 11: cp_async_wait<11>(); break;
+    case 12: cp_async_wait<12>(); break;
+    case 13: cp_async_wait<13>(); break;
+    case 14: cp_async_wait<14>(); break;
+    default: cp_async_wait<15>(); break;
+    }
+}
+
+// Fused i-axis stage, marching form (FP32): the maths of conv_i_fit_kernel with no
+// recomputed rows. Block: 32 threads along k x JB along j, one (j, k) column per
+// thread; blockIdx.z picks a chunk of `chunk` output rows along i. A thread streams
+// the input planes p = i0-2S .. i1+2S-1 of its column: each 16-byte cell goes through
+// a D-plane ring in shared memory by cp.async (zero filled outside the volume,
+// wrapped for the periodic boundary) and is added into the accumulators of the first
+// convolution (the four fields as two f32x2 pairs). Row m = p - S of that convolution
+// is then complete: (num, den, numb, denb) give f1, f2 and the pair
+// (l1 f1 - l2 f2, l1 f1^2 - l2 f2^2) (zero outside the volume unless periodic), which
+// is added into the accumulators of the second convolution, completing its output
+// row m - S. The march takes U planes per round: one barrier per round orders the
+// reads of the previous round's ring slots before their refill with planes U .. 2U-1
+// rounds ahead, and the U steps between barriers overlap one plane's division and
+// fit with the next plane's accumulation. f1 and f2 use the fast division (within
+// 2 ulp), the rest rounds as the scalar code does.
+// taps w[0] .. w[S] of a symmetric kernel, each as a float pair (w, w), passed by value
+// so that the kernel reads them from the parameter bank
+template <int S>
+struct TapPairs {
+    float2 w[S + 1];
+};
+
+template <int S, int JB, int D, int U, int MINB>
+__global__ void __launch_bounds__(32 * JB, MINB)
+    conv_i_fit_march_kernel(const float4* __restrict__ in, float2* __restrict__ out,
+                            float* f1_out, float* f2_out, Dims d, const TapPairs<S> tp,
+                            float l1, float l2, int chunk)
+{
+    constexpr int L = 2 * S + 1;
+    static_assert((D & (D - 1)) == 0 && D >= 2 * U && D <= 16, "ring: a power of two, >= 2U");
+    __shared__ __align__(16) float4 ring[D][JB][32];
+    const int k = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * JB + threadIdx.y;
+    const int i0 = blockIdx.z * chunk;
+    const int i1 = min(i0 + chunk, d.nx);
+    const bool col = k < d.nz && j < d.ny;
+    const int pa = i0 - 2 * S;
+    const int np = (i1 - i0) + 4 * S;
+    const long long cq = (long long)j * d.nz + k;        // this column in plane 0
+    const long long ps = (long long)d.ny * d.nz;         // plane stride
+    float4* const mine = &ring[0][threadIdx.y][threadIdx.x];
+    constexpr int SLOT = JB * 32;  // float4s between ring slots
+    auto issue = [&](int n) {
+        int i = 0;
+        const bool ok = col && n < np && d.halo(pa + n, d.nx, i);
+        const float4* src = ok ? in + (i * ps + cq) : in;
+        cp_async16_zfill(mine + (n & (D - 1)) * SLOT, src, ok);
+        cp_async_commit();
+    };
+    // planes 0 .. D-U-1 ahead of the first round
+#pragma unroll
+    for (int n = 0; n < D - U; ++n) issue(n);
+    const float2 (&w2)[S + 1] = tp.w;
+    // rows before the first one needed collect contributions and are never read
+    float2 a0[L], a1[L], bq[L];
+#pragma unroll
+    for (int t = 0; t < L; ++t) a0[t] = a1[t] = bq[t] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int n0 = 0; n0 < np; n0 += U) {
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            const int n = n0 + q;
+            // groups issued: planes 0 .. n0+D-U-1; plane n is complete when at most
+            // D-U-1-q of them are pending
+            cp_async_wait_n(D - U - 1 - q);
+            if (n < np) {
+                const float4 x = mine[(n & (D - 1)) * SLOT];
+                shift_conv2<S>(a0, w2, make_float2(x.x, x.y));
+                shift_conv2<S>(a1, w2, make_float2(x.z, x.w));
+                if (n >= 2 * S) {
+                    // row m = p - S of the first convolution is complete
+                    const int m = pa + n - S;
+                    const bool inside = m >= 0 && m < d.nx;
+                    float pv = 0.f, qv = 0.f;
+                    if (col && (inside || d.cyc)) {
+                        const float f1 = __fdividef(a0[0].x, a0[0].y);
+                        const float f2 = __fdividef(a1[0].x, a1[0].y);
+                        pv = f1 * l1 - f2 * l2;
+                        qv = (f1 * f1) * l1 - (f2 * f2) * l2;
+                        if (f1_out && inside && m >= i0 && m < i1) {
+                            const long long qq = m * ps + cq;
+                            f1_out[qq] = f1;
+                            f2_out[qq] = f2;
+                        }
+                    }
+                    // output row m - S is complete
+                    shift_conv2<S>(bq, w2, make_float2(pv, qv));
+                    if (n >= 4 * S && col) out[(m - S) * ps + cq] = bq[0];
+                }
+            }
+        }
+        // every thread has read this round's slots before the next rounds refill them
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < U; ++q) issue(n0 + D - U + q);
+    }
+    cp_async_wait<0>();
 }
 
 // Fused i-axis stage: K_i applied to the four stage-1 fields (H u0, H, Hb u0, Hb)
@@ -1178,18 +1473,6 @@ struct TbGeom {
     static constexpr int SLOTS = 3 * 2 * UPL;          // levels 1..3, double-buffered
     static constexpr size_t SMEM = (size_t)(U_RING + B_RING + SLOTS) * sizeof(float4);
 };
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 // blockIdx.x = tile (x fastest over packed columns), blockIdx.y = chunk of ci planes.
 template <int TJ, int TMV>

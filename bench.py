@@ -167,6 +167,60 @@ def bf16_peak_tflops():
     return 1590.0
 
 
+def unet_forward_ms(shape, dev, reps=5):
+    """Device time of one inference of the same network (layers as in
+    unet_flop_estimate, ReLU after each 3x3x3 convolution, 2x max-pooling down,
+    2x2x2 transposed convolutions up) run by the cuDNN convolutions behind torch.nn:
+    bf16 weights and activations, channels-last, random weights. A library network,
+    timed only to bound what a learned warm start could gain; it is not on the path."""
+    import torch
+    import torch.nn as nn
+
+    class Block(nn.Sequential):
+        def __init__(self, cin, cout):
+            super().__init__(nn.Conv3d(cin, cout, 3, padding=1), nn.ReLU(inplace=True),
+                             nn.Conv3d(cout, cout, 3, padding=1), nn.ReLU(inplace=True))
+
+    class UNet(nn.Module):
+        def __init__(self):
+            super().__init__()
+            self.e1, self.e2, self.e3 = Block(4, 16), Block(16, 32), Block(32, 64)
+            self.up2, self.up1 = nn.ConvTranspose3d(64, 32, 2, 2), nn.ConvTranspose3d(32, 16, 2, 2)
+            self.d2, self.d1 = Block(64, 32), Block(32, 16)
+            self.out = nn.Conv3d(16, 1, 1)
+
+        def forward(self, x):
+            a = self.e1(x)
+            b = self.e2(nn.functional.max_pool3d(a, 2))
+            c = self.e3(nn.functional.max_pool3d(b, 2))
+            b = self.d2(torch.cat([self.up2(c), b], 1))
+            return self.out(self.d1(torch.cat([self.up1(b), a], 1)))
+
+    prev = torch.backends.cudnn.benchmark
+    torch.backends.cudnn.benchmark = True
+    try:
+        net = UNet().to(dev, torch.bfloat16).to(memory_format=torch.channels_last_3d).eval()
+        x = torch.randn((1, 4) + tuple(shape), device=dev, dtype=torch.bfloat16)
+        x = x.contiguous(memory_format=torch.channels_last_3d)
+        with torch.inference_mode():
+            for _ in range(3):
+                net(x)
+            ts = []
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                net(x)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        del net, x
+        torch.cuda.empty_cache()
+        return sorted(ts)[len(ts) // 2]
+    finally:
+        torch.backends.cudnn.benchmark = prev
+
+
 def half_sweep_us(ctx, shape, dev, stream):
     """Device time of one red-black half-sweep inside a Poisson solve, in us."""
     import torch
@@ -362,7 +416,9 @@ def run_gpu(args):
         # an upper bound on its time-to-residual gain from measured numbers -- the plain
         # solve's device time per outer iteration against the network's FLOPs at the
         # measured dense bf16 peak, i.e. a perfect prediction (no sweeps after it) and a
-        # network at 100 % of that peak. Not a measurement of a built network.
+        # network at 100 % of that peak; and the same bound with the network's time
+        # measured on cuDNN's convolutions (random weights: the time does not depend on
+        # them). The project builds no network of its own.
         solve_ms = 0.0
         for k, (m, c) in prof.items():
             if k == "rb_half":
@@ -382,6 +438,14 @@ def run_gpu(args):
             "target": 2.0,
             "note": "bound from measured figures, no network is built",
         }
+        if not args.no_unet:
+            try:
+                cu_ms = unet_forward_ms(shape, dev)
+                learned["unet_ms_cudnn_bf16"] = cu_ms
+                learned["speedup_upper_bound_cudnn"] = solve_ms_iter / cu_ms
+                learned["unet_cudnn_tflops"] = unet_flop / (cu_ms * 1e-3) / 1e12
+            except Exception as exc:  # the bound above stands without it
+                learned["unet_cudnn_error"] = f"{type(exc).__name__}: {exc}"[:200]
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt_ms / args.steps, "higher_is_better": True,
@@ -564,6 +628,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-unet", action="store_true",
+                    help="skip timing the library network behind the warm-start bound")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batch"],
                     help="c2: one 256^3 volume per step (default); c3: 512x512x320 CT-like "
                          "volume, sigma 4, 200 iterations; batch: 48 uneven volumes")

@@ -96,6 +96,44 @@ def test_solve_mode_fp32_acceptance(ctx, pkg, O):
     assert pkg.synth.dice(got["phi"], want["phi"]) >= 0.999
 
 
+@pytest.mark.parametrize("shape,extra", [
+    ((37, 29, 45), dict(bc=2)),
+    ((70, 33, 21), dict(bc=1)),
+    ((45, 38, 52), dict(bc=2, sigma=4.0)),
+    ((33, 27, 30), dict(bc=2, conv_cyclic=1)),
+    ((26, 20, 36), dict(bc=1, conv_cyclic=1, sigma=4.0)),
+    ((40, 36, 34), dict(bc=2, lamda1=1.0, lamda2=2.0)),
+])
+def test_fp32_fit_stage_shapes(ctx, pkg, O, shape, extra):
+    """FP32 fitting stage (the i-axis march over chunks of planes) on ragged shapes,
+    both kernel widths and both convolution boundaries, against the FP64 checker."""
+    u0, phi0 = _case(pkg, shape, seed=3, r=min(shape) / 3.0)
+    got, want = _both(ctx, pkg, O, u0, phi0, dtype=np.float32, **{"maxiter": 4, **extra})
+    for key in ("u", "f1", "f2"):
+        assert rel(got[key], want[key]) <= 1e-5, key
+    assert pkg.synth.dice(got["phi"], want["phi"]) >= 0.999
+
+
+def test_fp32_fit_stage_chunking_bit_identical(pkg, monkeypatch):
+    """The i-axis march gives every output cell the same operations whatever the chunk
+    count, so the results are bit-identical for 1, 3 and 7 chunks and the cost model's
+    choice."""
+    u0, phi0 = _case(pkg, (75, 34, 40), seed=9, r=12.0)
+    params = pkg.default_params(**{**BASE, "maxiter": 3, "bc": 2})
+    outs = []
+    for chunks in ("1", "3", "7", "0"):
+        monkeypatch.setenv("IM3D_IFIT_CHUNKS", chunks)
+        c = pkg.Context(0)
+        try:
+            outs.append(c.rsfe_apply(u0.astype(np.float32), phi0.astype(np.float32), params,
+                                     want_u=True, want_f=True))
+        finally:
+            c.close()
+    for o in outs[1:]:
+        for key in ("phi", "u", "f1", "f2"):
+            assert np.array_equal(o[key], outs[0][key]), key
+
+
 def test_invalid_parameters_rejected(ctx, pkg):
     u0, phi0 = _case(pkg, (8, 8, 8))
     for bad in (dict(sigma=0.0), dict(lamda=-1.0), dict(dt=0.0), dict(epsilon=0.0),
