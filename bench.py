@@ -53,7 +53,6 @@ ALGO_BYTES_PER_VOXEL = {
     "conv_i_fit": 24.0,       # four fields read 16; the pair (l1 f1 - l2 f2, ...) write 8
     "conv_s_j2": 16.0,        # pair read 8, write 8
     "conv_k_rhs": 28.0,       # pair 8, u0 4, div(d-b) 4, phi 4 read; packed b_eff 4, u 4 write
-    "post_solve": 52.0,       # u 4, phiold 4, b 12, g 4 read; phi 4, b 12, d-b 12 write
     "div": 16.0,              # d-b read 12, div write 4
     "clamp_tol": 12.0,        # packed u read 4, phiold read 4, phi write 4
     "bregman": 44.0,          # phi 4, b 12, g 4 read; b 12, d-b 12 write
@@ -159,12 +158,13 @@ def unet_flop_estimate(shape):
 
 
 def bf16_peak_tflops():
+    """Dense bf16 peak (burst) in TFLOP/s and where it comes from."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         d = json.load(open(path))
         if "bf16_tflops" in d:
-            return float(d["bf16_tflops"])
-    return 1590.0
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
 
 
 def unet_forward_ms(shape, dev, reps=5):
@@ -427,12 +427,13 @@ def run_gpu(args):
                 solve_ms += m
         solve_ms_iter = solve_ms / max(kw["maxiter"], 1)
         unet_flop = unet_flop_estimate(shape)
-        bf16 = bf16_peak_tflops()
+        bf16, bf16_kind = bf16_peak_tflops()
         unet_ms = unet_flop / (bf16 * 1e12) * 1e3 if bf16 else None
         learned = {
             "plain_solve_ms_per_outer_iteration": solve_ms_iter,
             "unet_gflop_per_inference": unet_flop / 1e9,
             "bf16_peak_tflops": bf16,
+            "bf16_peak_source": bf16_kind + " (MEASURED_PEAKS.json bf16_tflops, cuBLAS burst)",
             "unet_ms_at_peak": unet_ms,
             "speedup_upper_bound": (solve_ms_iter / unet_ms) if unet_ms else None,
             "target": 2.0,
