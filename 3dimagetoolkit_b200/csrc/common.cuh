@@ -181,16 +181,31 @@ __device__ __forceinline__ void block_sum2_store(double a, double b, double* par
 }
 
 // sums[slot + v] = sum over b of part[v * nblocks + b], v < nvals, in a fixed order.
-__global__ void finalize_sums_kernel(const double* __restrict__ part, long long nblocks, int nvals,
-                                     double* sums, int slot)
+// One block of kFinThreads threads: thread t adds the slots b = t + m * kFinThreads in
+// four interleaved accumulators (m mod 4), so that four loads are in flight, then the
+// block adds the accumulators and the threads' sums in a fixed tree.
+constexpr int kFinThreads = 1024;
+__global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const double* __restrict__ part,
+                                                                    long long nblocks, int nvals,
+                                                                    double* sums, int slot)
 {
-    __shared__ double sm[256];
+    __shared__ double sm[kFinThreads];
     for (int v = 0; v < nvals; ++v) {
-        double acc = 0;
-        for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) acc += part[v * nblocks + b];
-        sm[threadIdx.x] = acc;
+        const double* pv = part + v * nblocks;
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        long long b = threadIdx.x;
+        for (; b + 3 * kFinThreads < nblocks; b += 4 * kFinThreads) {
+            a0 += pv[b];
+            a1 += pv[b + kFinThreads];
+            a2 += pv[b + 2 * kFinThreads];
+            a3 += pv[b + 3 * kFinThreads];
+        }
+        if (b < nblocks) a0 += pv[b];
+        if (b + kFinThreads < nblocks) a1 += pv[b + kFinThreads];
+        if (b + 2 * kFinThreads < nblocks) a2 += pv[b + 2 * kFinThreads];
+        sm[threadIdx.x] = (a0 + a1) + (a2 + a3);
         __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        for (int w = kFinThreads / 2; w > 0; w >>= 1) {
             if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
             __syncthreads();
         }

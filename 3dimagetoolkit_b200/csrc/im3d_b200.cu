@@ -659,7 +659,7 @@ int part_buf(im3d_ctx* ctx, dim3 grid, int nvals, double** out)
 int finalize(im3d_ctx* ctx, const double* part, dim3 grid, int nvals, int slot)
 {
     const long long nb = (long long)grid.x * grid.y * grid.z;
-    finalize_sums_kernel<<<1, 256, 0, ctx->stream>>>(part, nb, nvals, ctx->ctrl_d->sum, slot);
+    finalize_sums_kernel<<<1, kFinThreads, 0, ctx->stream>>>(part, nb, nvals, ctx->ctrl_d->sum, slot);
     return check_launch(ctx, "finalize_sums");
 }
 
