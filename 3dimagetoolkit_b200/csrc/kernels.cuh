@@ -736,6 +736,13 @@ __device__ __forceinline__ void cp_async_wait_n(int n)
     }
 }
 
+// taps w[0] .. w[S] of a symmetric kernel, each as a float pair (w, w), passed by value
+// so that the kernel reads them from the parameter bank
+template <int S>
+struct TapPairs {
+    float2 w[S + 1];
+};
+
 // Fused i-axis stage, marching form (FP32): the maths of conv_i_fit_kernel with no
 // recomputed rows. Block: 32 threads along k x JB along j, one (j, k) column per
 // thread; blockIdx.z picks a chunk of `chunk` output rows along i. A thread streams
@@ -747,17 +754,11 @@ __device__ __forceinline__ void cp_async_wait_n(int n)
 // (l1 f1 - l2 f2, l1 f1^2 - l2 f2^2) (zero outside the volume unless periodic), which
 // is added into the accumulators of the second convolution, completing its output
 // row m - S. The march takes U planes per round: one barrier per round orders the
-// reads of the previous round's ring slots before their refill with planes U .. 2U-1
-// rounds ahead, and the U steps between barriers overlap one plane's division and
-// fit with the next plane's accumulation. f1 and f2 use the fast division (within
-// 2 ulp), the rest rounds as the scalar code does.
-// taps w[0] .. w[S] of a symmetric kernel, each as a float pair (w, w), passed by value
-// so that the kernel reads them from the parameter bank
-template <int S>
-struct TapPairs {
-    float2 w[S + 1];
-};
-
+// reads of the previous round's ring slots before they are refilled, and the U steps
+// between barriers overlap one plane's division and fit with the next plane's
+// accumulation. Rounding differs from the tiled kernels by summation order only: each
+// row adds its 2S+1 products in plane order, where the tiled kernels add symmetric
+// pairs first; f1 and f2 use the fast division (within 2 ulp).
 template <int S, int JB, int D, int U, int MINB>
 __global__ void __launch_bounds__(32 * JB, MINB)
     conv_i_fit_march_kernel(const float4* __restrict__ in, float2* __restrict__ out,
