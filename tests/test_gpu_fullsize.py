@@ -8,7 +8,7 @@ CPU checker (which would take hours at these sizes):
   full runs are held to the segmentation bars (sign(phi - 0.5) agreement >= 99.9 %, Dice >=
   0.999) and to bounds on the field drift about three times what was measured on B200
   (256^3, 100 it.: u 9.2e-5, f1 2.0e-5, f2 2.9e-5; 512x512x320, 200 it.: u 1.8e-3, f1
-  5.0e-4, f2 4.3e-4, Dice 0.99967; an FP64 run at the same tolerance is itself 1.9e-5
+  5.0e-4, f2 4.2e-4, Dice 0.99967; an FP64 run at the same tolerance is itself 1.9e-5
   from a fully converged one at 256^3); the FP64 path is checked against the checker at
   smaller sizes;
 - every Poisson solve reached the relative residual it was asked for;
