@@ -439,7 +439,9 @@ def run_gpu(args):
             "target": 2.0,
             "note": "bound from measured figures, no network is built",
         }
-        if not args.no_unet:
+        # at N = 1 only, like the CPU baseline: the other ranks would wait at the final
+        # barrier meanwhile
+        if not args.no_unet and ws == 1:
             try:
                 cu_ms = unet_forward_ms(shape, dev)
                 learned["unet_ms_cudnn_bf16"] = cu_ms
