@@ -4,13 +4,18 @@ The package name starts with a digit, so import it with
 ``importlib.import_module("3dimagetoolkit_b200")``.
 
 * ``_abi``   -- ctypes binding of the C ABI (include/im3d_b200.h, libim3d_b200.so)
-* ``segm``, ``conv``, ``lapl``, ``im3d`` -- host-side mirror of the reference's classes
-  (rsfe_splitbregman, filtering, unsteady_poisson_functor, image3d) over that ABI
+* ``mhd``    -- headless MetaImage (.mhd/.raw) reader and writer
 * ``synth``  -- seeded synthetic volumes of the benchmark workloads
+* ``shard``  -- volumes of a batch across ranks
+
+The C++ mirror of the reference's classes (image3d, filtering,
+unsteady_poisson_functor, rsfe_splitbregman) is header-only, in include/im3d/.
 """
-from ._abi import (BC_DEFAULT, BC_DIR, BC_NEU, SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK, Context,
-                   Im3dError, RsfeParams, RsfeStats, default_params, lib)
+from ._abi import (BC_DEFAULT, BC_DIR, BC_NEU, OPT_DEVICE_MEMORY_LIMIT, OPT_FIT_CHUNKS,
+                   SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK, WS_OFF, WS_PREDICT, WS_TRAIN, Context, Im3dError,
+                   RsfeParams, RsfeStats, UNet, default_params, lib)
 from . import mhd, synth
 
 __all__ = ["Context", "Im3dError", "RsfeParams", "RsfeStats", "default_params", "lib", "mhd", "synth",
-           "BC_DEFAULT", "BC_DIR", "BC_NEU", "SWEEP_LEXICOGRAPHIC", "SWEEP_REDBLACK"]
+           "BC_DEFAULT", "BC_DIR", "BC_NEU", "SWEEP_LEXICOGRAPHIC", "SWEEP_REDBLACK",
+           "OPT_FIT_CHUNKS", "OPT_DEVICE_MEMORY_LIMIT", "UNet", "WS_OFF", "WS_PREDICT", "WS_TRAIN"]

@@ -27,12 +27,16 @@ ERR_NOT_CONVERGED = 3
 ERR_CUDA = 4
 ERR_OOM = 5
 ERR_NO_DEVICE = 6
+ERR_TOO_LARGE = 7
+ERR_NONFINITE = 8
 
 BC_DEFAULT, BC_NEU, BC_DIR = 0, 1, 2
 SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK = 0, 1
+OPT_FIT_CHUNKS, OPT_DEVICE_MEMORY_LIMIT = 1, 2
+WS_OFF, WS_PREDICT, WS_TRAIN = 0, 1, 2
 
 _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "NOT_CONVERGED", 4: "CUDA",
-                 5: "OOM", 6: "NO_DEVICE"}
+                 5: "OOM", 6: "NO_DEVICE", 7: "TOO_LARGE", 8: "NONFINITE"}
 
 
 class Im3dError(RuntimeError):
@@ -70,11 +74,23 @@ class RsfeStats(C.Structure):
         ("last_tol", C.c_double), ("last_rel_res", C.c_double), ("last_ls_err", C.c_double),
         ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_sweeps", C.c_int64),
         ("iterations", C.c_int32), ("last_sweeps", C.c_int32), ("not_converged", C.c_int32),
-        ("residual_checks", C.c_int32),
+        ("residual_checks", C.c_int32), ("ws_used", C.c_int32), ("ws_rejected", C.c_int32),
+        ("ws_loss", C.c_double),
     ]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Checkpoint(C.Structure):
+    """``im3d_rsfe_checkpoint``: the loop's state after outer iteration t."""
+
+    _fields_ = [("t", C.c_int32), ("init_variables", C.c_int32), ("sched_first", C.c_int32),
+                ("reserved", C.c_int32), ("sched_rate", C.c_double), ("tollerance", C.c_double),
+                ("phi", C.c_void_p), ("b", C.c_void_p), ("divdb", C.c_void_p)]
+
+
+OBSERVER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(Checkpoint))
 
 
 class VolumeDesc(C.Structure):
@@ -98,6 +114,7 @@ def lib() -> C.CDLL:
         L.im3d_ctx_last_error.restype = C.c_char_p
         L.im3d_ctx_launch_count.restype = C.c_int64
         L.im3d_rsfe_params_default.restype = None
+        L.im3d_unet_param_count.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -166,6 +183,10 @@ class Context:
         if st != OK:
             raise Im3dError(st, f"im3d_ctx_create(device={device}) failed")
         self.device = device
+        self._obs = None
+        self._obs_shape = ()
+        self._resume_keep = None
+        self._ws = None
 
     def close(self):
         if self._h:
@@ -216,6 +237,86 @@ class Context:
 
     def set_stream(self, stream_handle: int | None):
         self._check(lib().im3d_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def set_option(self, option: int, value: int):
+        """im3d_ctx_set_option: OPT_FIT_CHUNKS or OPT_DEVICE_MEMORY_LIMIT (bytes)."""
+        self._check(lib().im3d_ctx_set_option(self._h, C.c_int(option), C.c_int64(value)))
+
+    def set_observer(self, every: int, fn=None, with_state: bool = False, dtype=np.float64):
+        """Calls fn(state) after every ``every``-th outer iteration (not the last one) of
+        the next segmentations; state is a dict (t, tollerance, sched_first, sched_rate,
+        init_variables, phi[, b, divdb]) of numpy copies. fn returning True ends the
+        loop after that iteration. fn=None removes the observer. ``dtype`` is the
+        element type of the segmentations that follow."""
+        if fn is None:
+            self._obs = None
+            self._check(lib().im3d_ctx_set_observer(self._h, 0, 0, None, None))
+            return
+        dt = np.dtype(dtype)
+
+        def cb(_user, ck):
+            c = ck.contents
+            n = int(np.prod(self._obs_shape))
+
+            def arr(ptr, count, shape):
+                buf = (C.c_char * (count * dt.itemsize)).from_address(ptr)
+                return np.frombuffer(buf, dtype=dt, count=count).reshape(shape).copy()
+
+            st = dict(t=c.t, tollerance=c.tollerance, sched_first=c.sched_first,
+                      sched_rate=c.sched_rate, init_variables=c.init_variables,
+                      phi=arr(c.phi, n, self._obs_shape))
+            if c.b:
+                st["b"] = arr(c.b, 3 * n, (3,) + tuple(self._obs_shape))
+                st["divdb"] = arr(c.divdb, n, self._obs_shape)
+            try:
+                return 1 if fn(st) else 0
+            except Exception:  # an exception must not cross the C frame
+                return 1
+
+        self._obs = OBSERVER(cb)
+        self._check(lib().im3d_ctx_set_observer(self._h, C.c_int(every), C.c_int(int(with_state)),
+                                                self._obs, None))
+
+    def set_warm_start(self, net: "UNet | None", mode: int = WS_PREDICT, lr: float = 0.0):
+        """Learned warm start of the FP32 residual solves (WS_PREDICT, WS_TRAIN, WS_OFF)."""
+        self._ws = net
+        self._check(lib().im3d_ctx_set_warm_start(self._h, net.handle if net else None, C.c_int(mode),
+                                                  C.c_double(lr)))
+
+    def conv3d_bf16(self, x, w, bias=None, cin=None, c_off=0):
+        """One 3x3x3 convolution on the tensor cores: x a CUDA bfloat16 tensor
+        [N, D, H, W, C_pitch] (channels last), w FP32 [cout, cin, 3, 3, 3], bias FP32
+        [cout]; returns FP32 [N, D, H, W, cout]."""
+        import torch
+
+        nsamp, D, H, W, pitch = (int(v) for v in x.shape)
+        cout = int(w.shape[0])
+        cin = int(w.shape[1]) if cin is None else cin
+        w = w.to(device=x.device, dtype=torch.float32).contiguous()
+        b = None if bias is None else bias.to(device=x.device, dtype=torch.float32).contiguous()
+        out = torch.empty((nsamp, D, H, W, cout), dtype=torch.float32, device=x.device)
+        self._check(lib().im3d_conv3d_bf16(self._h, C.c_void_p(x.data_ptr()), C.c_int(pitch), C.c_int(c_off),
+                                           C.c_int(cin), C.c_void_p(w.data_ptr()),
+                                           C.c_void_p(b.data_ptr() if b is not None else 0), C.c_int(cout),
+                                           C.c_int(nsamp), C.c_int(D), C.c_int(H), C.c_int(W),
+                                           C.c_void_p(out.data_ptr())))
+        return out
+
+    def set_resume(self, state: dict | None):
+        """The next rsfe_apply starts from a state dict of set_observer(with_state=True)."""
+        if state is None:
+            self._check(lib().im3d_ctx_set_resume(self._h, None, C.c_int(0)))
+            self._resume_keep = None
+            return
+        phi = np.ascontiguousarray(state["phi"])
+        b = np.ascontiguousarray(state["b"], dtype=phi.dtype)
+        dv = np.ascontiguousarray(state["divdb"], dtype=phi.dtype)
+        ck = Checkpoint(t=state["t"], init_variables=state["init_variables"],
+                        sched_first=state["sched_first"], reserved=0,
+                        sched_rate=state["sched_rate"], tollerance=state["tollerance"],
+                        phi=phi.ctypes.data, b=b.ctypes.data, divdb=dv.ctypes.data)
+        self._resume_keep = (phi, b, dv)  # the arrays must live until the next apply
+        self._check(lib().im3d_ctx_set_resume(self._h, C.byref(ck), C.c_int(phi.dtype.itemsize)))
 
     # -- operators -----------------------------------------------------------
     def gauss_filter(self, x, sigma, h=(1.0, 1.0, 1.0), radius=3.0, pixel_approach=False, out=None,
@@ -320,8 +421,79 @@ class Context:
         f1 = _empty_like(myim) if want_f else None
         f2 = _empty_like(myim) if want_f else None
         st = RsfeStats()
+        self._obs_shape = tuple(int(x) for x in myim.shape)
         fn = getattr(lib(), "im3d_rsfe_apply_" + _suffix(dt))
-        self._check(fn(self._h, pm, pi, *map(C.c_int, myim.shape), *map(C.c_double, h),
-                       C.byref(p), _ptr(phi)[0], _ptr(u)[0], _ptr(f1)[0], _ptr(f2)[0],
-                       C.byref(st)))
+        try:
+            self._check(fn(self._h, pm, pi, *map(C.c_int, myim.shape), *map(C.c_double, h),
+                           C.byref(p), _ptr(phi)[0], _ptr(u)[0], _ptr(f1)[0], _ptr(f2)[0],
+                           C.byref(st)))
+        finally:
+            self._resume_keep = None
         return dict(phi=phi, u=u, f1=f1, f2=f2, stats=st.as_dict())
+
+
+class UNet:
+    """The learned warm start's network (im3d_unet_*): a 3-level 3-D U-Net whose
+    forward and backward passes run on the library's tensor-core kernels."""
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        ctx._check(lib().im3d_unet_create(ctx.handle, C.c_uint64(seed), C.byref(self._h)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().im3d_unet_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def param_count(self) -> int:
+        return int(lib().im3d_unet_param_count(self._h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.param_count, dtype=np.float32)
+        self.ctx._check(lib().im3d_unet_get_params(self.ctx.handle, self._h, out.ctypes.data_as(C.c_void_p),
+                                                   C.c_int64(out.size)))
+        return out
+
+    def set_params(self, flat):
+        flat = np.ascontiguousarray(flat, dtype=np.float32)
+        self.ctx._check(lib().im3d_unet_set_params(self.ctx.handle, self._h, flat.ctypes.data_as(C.c_void_p),
+                                                   C.c_int64(flat.size)))
+
+    def forward(self, x):
+        """x: [nsamp, 4, nx, ny, nz] FP32 (numpy or CUDA tensor) -> y [nsamp, nx, ny, nz]."""
+        px, dt = _ptr(x)
+        ns, _, nx, ny, nz = (int(v) for v in x.shape)
+        y = _empty_like(x, (ns, nx, ny, nz))
+        self.ctx._check(lib().im3d_unet_forward(self.ctx.handle, self._h, px, C.c_int(ns), C.c_int(nx),
+                                                C.c_int(ny), C.c_int(nz), _ptr(y)[0]))
+        return y
+
+    def train_step(self, x, target, lr: float, want_grads: bool = False):
+        """One Adam step on (x, target); returns the loss (and the FP32 gradients)."""
+        px, _ = _ptr(x)
+        pt, _ = _ptr(target)
+        ns, _, nx, ny, nz = (int(v) for v in x.shape)
+        loss = C.c_double(0)
+        g = np.empty(self.param_count, dtype=np.float32) if want_grads else None
+        self.ctx._check(lib().im3d_unet_train_step(self.ctx.handle, self._h, px, pt, C.c_int(ns), C.c_int(nx),
+                                                   C.c_int(ny), C.c_int(nz), C.c_double(lr), C.byref(loss),
+                                                   g.ctypes.data_as(C.c_void_p) if g is not None else None))
+        return (float(loss.value), g) if want_grads else float(loss.value)

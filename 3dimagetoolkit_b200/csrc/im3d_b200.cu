@@ -20,6 +20,7 @@
 
 #include "../../include/im3d_b200.h"
 #include "common.cuh"
+#include "internal.h"
 #include "kernels.cuh"
 
 using namespace im3d;
@@ -55,15 +56,24 @@ struct im3d_ctx {
     std::vector<std::pair<std::string, Acc>> prof_acc;
     // worker contexts of the batched entry points (own stream and buffers each)
     std::vector<im3d_ctx*> workers;
-    // L2 set-aside for the Gauss-Seidel state (per-context limit, released on destroy)
-    size_t persist_max = 0;
-    size_t window_max = 0;
-    bool persist_set = false;
-    // temporally blocked sweep pairs for FP32 solves (opt-in: IM3D_TB=1)
-    bool tb_enabled = false;
-    int pair_resident[2] = {0, 0};  // resident rb_pair_kernel CTAs (24- and 22-row tiles)
     int num_sms = 148;
     int ifit_chunks = 0;  // i chunks of the marching fit stage (0: cost model)
+    size_t mem_limit = 0;  // device bytes the context may hold in buffers (0: no limit)
+    size_t mem_held = 0;   // device bytes it holds in buffers now
+    // per-iteration observer (im3d_ctx_set_observer) and its host copy of the state
+    im3d_rsfe_observer obs = nullptr;
+    void* obs_user = nullptr;
+    int obs_every = 0;
+    int obs_state = 0;
+    std::vector<unsigned char> obs_host;
+    // learned warm start of the Poisson solves (im3d_ctx_set_warm_start)
+    im3d_unet* ws_net = nullptr;
+    int ws_mode = IM3D_WS_OFF;
+    double ws_lr = 0;
+    // pending resume of the next segmentation (im3d_ctx_set_resume)
+    bool resume = false;
+    int resume_esize = 0;
+    im3d_rsfe_checkpoint resume_from{};
     long long residual_checks = 0;  // rb_check calls, for the statistics
 };
 
@@ -162,7 +172,17 @@ int buf(im3d_ctx* ctx, const char* name, size_t bytes, void** out, bool zero = f
 {
     DevBuf& b = ctx->bufs[name];
     if (b.bytes < bytes) {
+        // the context's memory budget (IM3D_OPT_DEVICE_MEMORY_LIMIT) is checked before
+        // anything is freed or allocated
+        if (ctx->mem_limit && ctx->mem_held - b.bytes + bytes > ctx->mem_limit) {
+            ctx->err = std::string("device memory limit of the context (") +
+                       std::to_string(ctx->mem_limit) + " bytes) reached: buffer " + name + " needs " +
+                       std::to_string(bytes) + " bytes, " + std::to_string(ctx->mem_held - b.bytes) +
+                       " are held";
+            return IM3D_ERR_OOM;
+        }
         if (b.p) cudaFree(b.p);
+        ctx->mem_held -= b.bytes;
         b.p = nullptr;
         b.bytes = 0;
         cudaError_t e = cudaMalloc(&b.p, bytes);
@@ -173,6 +193,7 @@ int buf(im3d_ctx* ctx, const char* name, size_t bytes, void** out, bool zero = f
             return IM3D_ERR_OOM;
         }
         b.bytes = bytes;
+        ctx->mem_held += bytes;
     }
     if (zero) IM3D_CUDA(ctx, cudaMemsetAsync(b.p, 0, bytes, ctx->stream));
     *out = b.p;
@@ -443,7 +464,7 @@ int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T*
 // The kernel is issue-bound, so the chunk count minimises the planes one SM streams:
 // ceil(blocks / SMs) x (chunk + 4S), where each chunk re-streams 4S halo planes
 // (measured at 256^3: 1, 2, 3, 4 chunks take 152, 144, 160, 164 us; this picks 2).
-// IM3D_IFIT_CHUNKS overrides it.
+// The context option IM3D_OPT_FIT_CHUNKS overrides it.
 template <int S>
 int pass_i_fit_march(im3d_ctx* ctx, const Vec<float, 4>* in, Vec<float, 2>* out, float* f1,
                      float* f2, const Dims& d, const float* hw, float l1, float l2)
@@ -699,97 +720,6 @@ int read_ctrl(im3d_ctx* ctx)
     return sync(ctx);
 }
 
-// Keeps the colour-packed Gauss-Seidel state resident in L2 during a solve: a
-// persisting access-policy window on the context's stream over U (b_eff, read once per
-// sweep, streams). The set-aside is a limit of this context only; it is released by
-// l2_unpin and on im3d_ctx_destroy.
-void l2_pin(im3d_ctx* ctx, const void* base, size_t bytes)
-{
-    if (ctx->persist_max == 0 || ctx->window_max == 0) return;
-    if (!ctx->persist_set) {
-        if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, ctx->persist_max) != cudaSuccess) {
-            cudaGetLastError();
-            ctx->persist_max = 0;
-            return;
-        }
-        ctx->persist_set = true;
-    }
-    cudaStreamAttrValue at = {};
-    at.accessPolicyWindow.base_ptr = const_cast<void*>(base);
-    at.accessPolicyWindow.num_bytes = bytes < ctx->window_max ? bytes : ctx->window_max;
-    const double ratio = (double)ctx->persist_max / (double)at.accessPolicyWindow.num_bytes;
-    at.accessPolicyWindow.hitRatio = (float)(ratio < 1.0 ? ratio : 1.0);
-    at.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-    at.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-    if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &at) != cudaSuccess)
-        cudaGetLastError();
-}
-
-void l2_unpin(im3d_ctx* ctx)
-{
-    if (!ctx->persist_set) return;
-    cudaStreamAttrValue at = {};
-    at.accessPolicyWindow.num_bytes = 0;
-    if (cudaStreamSetAttribute(ctx->stream, cudaStreamAttributeAccessPolicyWindow, &at) != cudaSuccess)
-        cudaGetLastError();
-    if (cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
-}
-
-// Two red-black sweeps in one temporally blocked pass (rb_pair_kernel, FP32).
-// Tiles of 8 float4 columns (32 packed cells) by 24 or 22 rows; the tile height and
-// the chunk of planes per CTA are chosen to minimise the work of the busiest SM,
-// ceil(ctas / resident) * (chunk + 8) * threads per CTA, so that the CTAs fill whole
-// waves of the GPU.
-template <int TJ>
-int rb_pair_plan(im3d_ctx* ctx, const Dims& d, int slot, long long* cost, int* ci_out)
-{
-    using G = TbGeom<TJ, 8>;
-    auto kern = rb_pair_kernel<TJ, 8>;
-    if (ctx->pair_resident[slot] <= 0) {
-        IM3D_TRY(set_smem(ctx, kern, G::SMEM));
-        int per_sm = 0;
-        IM3D_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, G::NT, G::SMEM));
-        if (per_sm < 1) return fail(ctx, IM3D_ERR_CUDA, "rb_pair_kernel does not fit on an SM");
-        ctx->pair_resident[slot] = per_sm * ctx->num_sms;
-    }
-    const long long tiles = (long long)((d.hz() + 31) / 32) * ((d.ny + TJ - 1) / TJ);
-    *cost = -1;
-    for (int ci = 8; ci <= d.nx; ++ci) {
-        const long long chunks = (d.nx + ci - 1) / ci;
-        const long long waves = (tiles * chunks + ctx->pair_resident[slot] - 1) / ctx->pair_resident[slot];
-        const long long cst = waves * (ci + 8) * G::NT;
-        if (*cost < 0 || cst < *cost) {
-            *cost = cst;
-            *ci_out = ci;
-        }
-    }
-    return IM3D_OK;
-}
-
-template <int TJ>
-int rb_pair_launch(im3d_ctx* ctx, const float* Uin, float* Uout, const float* B, const Dims& d,
-                   const GsCoef<float>& c, int ci)
-{
-    using G = TbGeom<TJ, 8>;
-    const long long tiles = (long long)((d.hz() + 31) / 32) * ((d.ny + TJ - 1) / TJ);
-    const dim3 grid((unsigned)tiles, (unsigned)((d.nx + ci - 1) / ci));
-    const int pf = prof_begin(ctx, "rb_pair");
-    rb_pair_kernel<TJ, 8><<<grid, G::NT, G::SMEM, ctx->stream>>>(Uin, Uout, B, d, c, ci);
-    prof_end(ctx, pf);
-    return check_launch(ctx, "rb_pair");
-}
-
-int rb_pair_pass(im3d_ctx* ctx, const float* Uin, float* Uout, const float* B, const Dims& d,
-                 const GsCoef<float>& c)
-{
-    long long c24 = 0, c22 = 0;
-    int ci24 = 0, ci22 = 0;
-    IM3D_TRY(rb_pair_plan<24>(ctx, d, 0, &c24, &ci24));
-    IM3D_TRY(rb_pair_plan<22>(ctx, d, 1, &c22, &ci22));
-    if (c22 < c24) return rb_pair_launch<22>(ctx, Uin, Uout, B, d, c, ci22);
-    return rb_pair_launch<24>(ctx, Uin, Uout, B, d, c, ci24);
-}
-
 // FP64 residual of the packed state, and sum b_eff^2 on the first call (*beff2 < 0);
 // returns the relative residual in *rel.
 template <typename T>
@@ -832,49 +762,6 @@ int rb_solve(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
     if (rate_out) *rate_out = rate_hint;
     *conv = false;
     *rel = -1;
-    l2_pin(ctx, U, 2 * (size_t)d.npk() * sizeof(T));
-    struct Unpin {
-        im3d_ctx* c;
-        ~Unpin() { l2_unpin(c); }
-    } unpin{ctx};
-    // FP32 with omega == 1: sweeps go in temporally blocked pairs; checks land on pair
-    // boundaries (at most one sweep past the scheduled one)
-    if constexpr (std::is_same<T, float>::value) {
-        if (omega == 1.0 && ctx->tb_enabled && max_sweeps >= 2) {
-            const size_t cnt = 2 * (size_t)d.npk();
-            T* alt = nullptr;
-            IM3D_TRY(tbuf<T>(ctx, "upk_alt", cnt, &alt));
-            T* cur = U;
-            T* nxt = alt;
-            bool done = false;
-            while (s + 2 <= max_sweeps) {
-                IM3D_TRY(rb_pair_pass(ctx, cur, nxt, B, d, c));
-                std::swap(cur, nxt);
-                s += 2;
-                if (s < next && s != max_sweeps) continue;
-                double r = 0;
-                IM3D_TRY(rb_check<T>(ctx, cur, B, d, c, &beff2, &r));
-                *rel = r;
-                if (r <= tol) {
-                    *conv = true;
-                    done = true;
-                    break;
-                }
-                next = next_check(s, r, s_prev, r_prev, tol, check_every, rate_hint, &rate_used);
-                if (next > max_sweeps) next = max_sweeps;
-                s_prev = s;
-                r_prev = r;
-            }
-            if (rate_out) *rate_out = rate_used > 0 ? rate_used : rate_hint;
-            if (cur != U)
-                IM3D_CUDA(ctx, cudaMemcpyAsync(U, cur, cnt * sizeof(T), cudaMemcpyDeviceToDevice,
-                                               ctx->stream));
-            if (done || s == max_sweeps) {
-                *sweeps = s;
-                return IM3D_OK;
-            }
-        }
-    }
     while (s < max_sweeps) {
         IM3D_TRY(rb_sweep(ctx, U, B, d, c, 0, omega));
         ++s;
@@ -906,15 +793,17 @@ double order_key_to_double(unsigned long long k)
     return v;
 }
 
+// *nonfinite (may be NULL) receives whether any value is NaN or Inf.
 template <typename T>
-int minmax(im3d_ctx* ctx, const T* p, long long n, T* mn, T* mx)
+int minmax(im3d_ctx* ctx, const T* p, long long n, T* mn, T* mx, bool* nonfinite = nullptr)
 {
-    IM3D_CUDA(ctx, cudaMemsetAsync(ctx->ctrl_d->umax, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    IM3D_CUDA(ctx, cudaMemsetAsync(ctx->ctrl_d->umax, 0, 4 * sizeof(unsigned long long), ctx->stream));
     minmax_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(p, n, ctx->ctrl_d->umax);
     IM3D_TRY(check_launch(ctx, "minmax"));
     IM3D_TRY(read_ctrl(ctx));
     *mx = (T)order_key_to_double(ctx->ctrl_h->umax[0]);
     *mn = (T)(-order_key_to_double(ctx->ctrl_h->umax[1]));
+    if (nonfinite) *nonfinite = ctx->ctrl_h->umax[3] != 0;
     return IM3D_OK;
 }
 
@@ -1052,6 +941,67 @@ int extract_cc(im3d_ctx* ctx, T* phi, const Dims& d, double hx, double hy, doubl
     return IM3D_OK;
 }
 
+// ------------------------------------------------------- learned warm start
+// The fields of one solve, gathered for the network (FP32 only).
+struct WsBufs {
+    float* x;      // 4 input volumes
+    float* y;      // the network's correction / the training target
+    float* upk0;   // the solve's start (packed u_in)
+};
+
+int ws_status(im3d_ctx* ctx, int st)
+{
+    if (st != IM3D_OK && ctx->err.empty()) ctx->err = "learned warm start failed";
+    return st;
+}
+
+// Before a solve: IM3D_WS_PREDICT adds the network's correction to u_in when that
+// lowers the residual; both modes keep u_in in w.upk0.
+int ws_before(im3d_ctx* ctx, const Dims& d, const GsCoef<float>& c, float* upk, const float* bpk,
+              const float* prevu, const float* divdb, const float* phi, float inv_dt, int dirichlet,
+              const WsBufs& w, int* used, int* rejected)
+{
+    ws_fields_kernel<<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(bpk, upk, prevu, divdb, phi, d, inv_dt, w.x);
+    IM3D_TRY(check_launch(ctx, "ws_fields"));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(w.upk0, upk, 2 * (size_t)d.npk() * sizeof(float), cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+    if (ctx->ws_mode != IM3D_WS_PREDICT) return IM3D_OK;
+    const int pf = prof_begin(ctx, "ws_network");
+    const long long l0 = im3d::unet::launch_total();
+    IM3D_TRY(ws_status(ctx, im3d::unet::net_forward_fields(ctx->ws_net, ctx->stream, w.x, 1, d.nx, d.ny, d.nz, w.y,
+                                                            ctx->err)));
+    ctx->launches += im3d::unet::launch_total() - l0;
+    prof_end(ctx, pf);
+    double beff2 = -1, r0 = 0, r1 = 0;
+    IM3D_TRY(rb_check<float>(ctx, upk, bpk, d, c, &beff2, &r0));
+    ws_apply_kernel<<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(upk, w.y, d, dirichlet);
+    IM3D_TRY(check_launch(ctx, "ws_apply"));
+    IM3D_TRY(rb_check<float>(ctx, upk, bpk, d, c, &beff2, &r1));
+    if (r1 < r0) {
+        ++*used;
+    } else {
+        IM3D_CUDA(ctx, cudaMemcpyAsync(upk, w.upk0, 2 * (size_t)d.npk() * sizeof(float), cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+        ++*rejected;
+    }
+    return IM3D_OK;
+}
+
+// After a solve (IM3D_WS_TRAIN): one training step on the solve's fields and the
+// correction it made.
+int ws_after(im3d_ctx* ctx, const Dims& d, const float* upk, const WsBufs& w, double* loss)
+{
+    ws_target_kernel<<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(upk, w.upk0, d, w.y);
+    IM3D_TRY(check_launch(ctx, "ws_target"));
+    const int pf = prof_begin(ctx, "ws_train");
+    const long long l0 = im3d::unet::launch_total();
+    IM3D_TRY(ws_status(ctx, im3d::unet::net_train_fields(ctx->ws_net, ctx->stream, w.x, w.y, nullptr, 1, d.nx, d.ny,
+                                                          d.nz, ctx->ws_lr, loss, nullptr, ctx->err)));
+    ctx->launches += im3d::unet::launch_total() - l0;
+    prof_end(ctx, pf);
+    return IM3D_OK;
+}
+
 // --------------------------------------------------------------- the loop
 template <typename T>
 struct Outs {
@@ -1087,6 +1037,20 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     if (!(p->b0 > p->a0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "b0 has to be greater than a0");
     if (p->gs_rel_res_tol > 0 && !(p->omega > 0 && p->omega < 2))
         return fail(ctx, IM3D_ERR_INVALID_ARG, "omega must lie in (0, 2)");
+    const bool ws = ctx->ws_net && ctx->ws_mode != IM3D_WS_OFF && p->gs_rel_res_tol > 0;
+    if (ws && !std::is_same<T, float>::value)
+        return fail(ctx, IM3D_ERR_UNSUPPORTED, "the learned warm start runs with the FP32 entry point");
+
+    // a pending resume is consumed by this call, whatever its outcome
+    const bool resuming = ctx->resume;
+    const im3d_rsfe_checkpoint from = ctx->resume_from;
+    ctx->resume = false;
+    if (resuming) {
+        if (ctx->resume_esize != (int)sizeof(T))
+            return fail(ctx, IM3D_ERR_INVALID_ARG, "the checkpoint's element size does not match this call");
+        if (!from.phi || !from.b || !from.divdb || from.t < 0)
+            return fail(ctx, IM3D_ERR_INVALID_ARG, "a checkpoint needs phi, b, divdb and t >= 0");
+    }
 
     IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     // the convolution passes take the plug-in's boundary; no other kernel reads cyc
@@ -1104,7 +1068,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     const T* u0 = nullptr;
     const T* init = nullptr;
     IM3D_TRY(dev_in<T>(ctx, myim_user, n, "in_myim", &u0));
-    if (init_user) IM3D_TRY(dev_in<T>(ctx, init_user, n, "in_init", &init));
+    if (init_user && !resuming) IM3D_TRY(dev_in<T>(ctx, init_user, n, "in_init", &init));
 
     T *phiA, *phiB, *g, *divdb, *b3, *dmb, *kones = nullptr, *rhs = nullptr, *upk = nullptr,
       *bpk = nullptr, *prev = nullptr;
@@ -1133,27 +1097,64 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     IM3D_TRY(dev_out<T>(ctx, f2_user, n, "out_f2", &f2_d));
     if (f1_d && !f2_d) IM3D_TRY(tbuf<T>(ctx, "out_f2", n, &f2_d));
     if (f2_d && !f1_d) IM3D_TRY(tbuf<T>(ctx, "out_f1", n, &f1_d));
-
-    // initial level set (rsfe_splitbregman_imp.hxx:99-170 / :48-95), then
-    // change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636)
-    if (init) {
-        IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, init, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
-    } else {
-        const int ix = (int)(nx * 0.33), iy = (int)(ny * 0.33), iz = (int)(nz * 0.33);
-        const int fx = (int)(nx * (1 - 0.33)), fy = (int)(ny * (1 - 0.33)), fz = (int)(nz * (1 - 0.33));
-        cube_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(phiA, d, ix, iy, iz, fx,
-                                                                           fy, fz, a0, b0);
-        IM3D_TRY(check_launch(ctx, "cube"));
+    WsBufs wsb{nullptr, nullptr, nullptr};
+    int ws_used = 0, ws_rejected = 0, ws_steps = 0;
+    double ws_loss = 0;
+    if (ws) {
+        IM3D_TRY(tbuf<float>(ctx, "ws_x", 4 * (size_t)n, &wsb.x));
+        IM3D_TRY(tbuf<float>(ctx, "ws_y", (size_t)n, &wsb.y));
+        IM3D_TRY(tbuf<float>(ctx, "ws_upk0", (size_t)npk2, &wsb.upk0));
+        // the previous solve's u: the clamp kernel writes it (before the clamp)
+        if (!u_d) IM3D_TRY(tbuf<T>(ctx, "ws_prevu", n, &u_d));
     }
+
+    IM3D_TRY(zero_ctrl(ctx));
     {
-        IM3D_TRY(zero_ctrl(ctx));
+        // NaN or Inf in the image: refused here (the reference's debug build traps the
+        // floating-point exception they raise, exceptions.hxx:25-35)
         T mn, mx;
-        IM3D_TRY(minmax<T>(ctx, phiA, n, &mn, &mx));
+        bool bad = false;
+        IM3D_TRY(minmax<T>(ctx, u0, n, &mn, &mx, &bad));
+        if (bad) return fail(ctx, IM3D_ERR_NONFINITE, "myim holds NaN or Inf values");
+    }
+    int t0 = 0;  // outer iterations already done (a resumed run)
+    double tollerance = 1000;
+    int init_variables = p->init_variables;
+    int sched_first = 0;  // residual schedule carried between Poisson solves
+    double sched_rate = 0;
+    if (resuming) {
+        // the state of the checkpoint instead of the initial level set
+        IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, from.phi, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(b3, from.b, 3 * n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(divdb, from.divdb, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        t0 = from.t;
+        tollerance = from.tollerance;
+        init_variables = from.init_variables;
+        sched_first = from.sched_first;
+        sched_rate = from.sched_rate;
+    } else {
+        // initial level set (rsfe_splitbregman_imp.hxx:99-170 / :48-95), then
+        // change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636)
+        if (init) {
+            IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, init, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+        } else {
+            const int ix = (int)(nx * 0.33), iy = (int)(ny * 0.33), iz = (int)(nz * 0.33);
+            const int fx = (int)(nx * (1 - 0.33)), fy = (int)(ny * (1 - 0.33)), fz = (int)(nz * (1 - 0.33));
+            cube_kernel<T><<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(phiA, d, ix, iy, iz, fx,
+                                                                               fy, fz, a0, b0);
+            IM3D_TRY(check_launch(ctx, "cube"));
+        }
+        T mn, mx;
+        bool bad = false;
+        IM3D_TRY(minmax<T>(ctx, phiA, n, &mn, &mx, &bad));
+        if (bad) return fail(ctx, IM3D_ERR_NONFINITE, "init holds NaN or Inf values");
         const T shifted_max = mx - mn;
         const T s = shifted_max / (T)(b0 - a0);
         affine_kernel<T><<<flat_grid(n), 256, 0, ctx->stream>>>(phiA, n, mn, s, a0);
         IM3D_TRY(check_launch(ctx, "affine"));
     }
+    // the first solve's "previous u" is the initial level set
+    if (ws) IM3D_CUDA(ctx, cudaMemcpyAsync(u_d, phiA, n * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
 
     // filters, kones (only used when lamda1 != lamda2), edge detector
     Taps<T> tp;
@@ -1180,18 +1181,14 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     const T center = (T)((p->a0 + p->b0) / 2.);
     const T inv_eps = (T)(1.0 / p->epsilon);
     const double hhh = hx * hy * hz;
-    double tollerance = 1000;
-    int init_variables = p->init_variables;
     long long total_sweeps = 0;
     int last_sweeps = 0, not_conv = 0, t;
-    int sched_first = 0;  // residual schedule carried between Poisson solves
     const long long checks0 = ctx->residual_checks;
-    double sched_rate = 0;
     double last_rel = -1, last_ls_err = -1;
     T* phi = phiA;   // current level set (natural)
     T* other = phiB;
 
-    for (t = 1; tollerance > p->tol && t <= p->maxiter; ++t) {
+    for (t = t0 + 1; tollerance > p->tol && t <= p->maxiter; ++t) {
         // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
         IM3D_TRY((pass_k<T, 4>(ctx, LdHeaviside<T>{phi, u0, d, center, inv_eps}, StVec<T, 4>{W1, d},
                                d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
@@ -1227,9 +1224,22 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             // check after as many sweeps as it needed, its contraction rate as the first
             // prediction (the sweep counts of consecutive solves differ by a sweep or two)
             double rate = 0;
+            if constexpr (std::is_same<T, float>::value) {
+                if (ws)
+                    IM3D_TRY(ws_before(ctx, d, coef, upk, bpk, u_d, divdb, phi, (float)(1.0 / p->dt), neu ? 0 : 1,
+                                       wsb, &ws_used, &ws_rejected));
+            }
             IM3D_TRY(rb_solve<T>(ctx, upk, bpk, d, coef, p->gs_rel_res_tol, p->gs_max_sweeps,
                                  p->gs_check_every, p->omega, &sw, &rel, &conv, sched_first,
                                  sched_rate, &rate));
+            if constexpr (std::is_same<T, float>::value) {
+                if (ws && ctx->ws_mode == IM3D_WS_TRAIN) {
+                    double l = 0;
+                    IM3D_TRY(ws_after(ctx, d, upk, wsb, &l));
+                    ws_loss += l;
+                    ++ws_steps;
+                }
+            }
             sched_first = conv ? sw : 0;
             sched_rate = conv ? rate : 0;
             if (!conv) not_conv++;
@@ -1354,6 +1364,32 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         tollerance = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_DPHI2]) /
                      std::sqrt(hhh * ctx->ctrl_h->sum[SUM_PHIOLD2]);
         if (lex) std::swap(phi, other);
+        // dumps and checkpoints: the reference's rule t % dumpfrequency == 0, t != maxiter
+        // (rsfe_splitbregman_imp.hxx:1940-1951)
+        if (ctx->obs && ctx->obs_every > 0 && t % ctx->obs_every == 0 && t != p->maxiter) {
+            const size_t nb = (size_t)n * sizeof(T);
+            ctx->obs_host.resize(ctx->obs_state ? 5 * nb : nb);
+            T* hp = reinterpret_cast<T*>(ctx->obs_host.data());
+            IM3D_CUDA(ctx, cudaMemcpyAsync(hp, phi, nb, cudaMemcpyDeviceToHost, ctx->stream));
+            if (ctx->obs_state) {
+                IM3D_CUDA(ctx, cudaMemcpyAsync(hp + n, b3, 3 * nb, cudaMemcpyDeviceToHost, ctx->stream));
+                IM3D_CUDA(ctx, cudaMemcpyAsync(hp + 4 * n, divdb, nb, cudaMemcpyDeviceToHost, ctx->stream));
+            }
+            IM3D_TRY(sync(ctx));
+            im3d_rsfe_checkpoint ck{};
+            ck.t = t;
+            ck.init_variables = init_variables;
+            ck.sched_first = sched_first;
+            ck.sched_rate = sched_rate;
+            ck.tollerance = tollerance;
+            ck.phi = hp;
+            ck.b = ctx->obs_state ? hp + n : nullptr;
+            ck.divdb = ctx->obs_state ? hp + 4 * n : nullptr;
+            if (ctx->obs(ctx->obs_user, &ck) != 0) {
+                ++t;  // the loop ends after this iteration, as with end_now
+                break;
+            }
+        }
     }
     IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
 
@@ -1377,6 +1413,9 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
         stats->last_ls_err = last_ls_err;
         stats->not_converged = not_conv;
         stats->residual_checks = (int32_t)(ctx->residual_checks - checks0);
+        stats->ws_used = ws_used;
+        stats->ws_rejected = ws_rejected;
+        stats->ws_loss = ws_steps ? ws_loss / ws_steps : 0.0;
         float ms = 0;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
         stats->setup_ms = ms;
@@ -1571,6 +1610,34 @@ float* noalloc_scratch_address(int device, cudaError_t* err)
     return addr[device];
 }
 
+// A device pointer of the current device (the kernels would otherwise touch another
+// GPU's memory, which faults without peer access).
+bool on_current_device(const void* p, int device)
+{
+    cudaPointerAttributes a;
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
+}
+
+// One launch on the caller's stream; the launch's own status is returned, so the call
+// reports its errors without reading (and clearing) an error the caller left pending.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_on(cudaStream_t stream, void (*kern)(KArgs...), dim3 grid, dim3 blk, size_t smem,
+                      Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = blk;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) cudaGetLastError();  // the error this launch raised
+    return e;
+}
+
 int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, double hx,
                          double hy, double hz, double sigma, double radius, int pixel_approach,
                          cudaStream_t stream)
@@ -1579,9 +1646,16 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
     if (nz == 1 || nx < 3 || ny < 3 || nz < 3) return IM3D_ERR_UNSUPPORTED;
     if (!(hx > 0) || !(hy > 0) || !(hz > 0) || !(sigma > 0) || !(radius > 0))
         return IM3D_ERR_INVALID_ARG;
+    // the launch geometry of the j and i passes puts nx and ny on grid.z
+    if (nx > 65535 || ny > 65535) return IM3D_ERR_INVALID_ARG;
     const Dims d{nx, ny, nz};
     if (d.n() > kNoAllocMaxVoxels) return IM3D_ERR_TOO_LARGE;
-    if (!is_device_ptr(in) || !is_device_ptr(out)) return IM3D_ERR_INVALID_ARG;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return IM3D_ERR_CUDA;
+    }
+    if (!on_current_device(in, device) || !on_current_device(out, device)) return IM3D_ERR_INVALID_ARG;
     // taps on the host stack: conv::filtering<T>::build_gaussian_filter per axis
     NoAllocTaps taps;
     int nh[3];
@@ -1602,11 +1676,6 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
         }
         for (int t = 0; t < NH_MAX; ++t) taps.w[a * NH_MAX + t] = t < m ? (float)(w[t] / sum) : 0.f;
     }
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) {
-        cudaGetLastError();
-        return IM3D_ERR_CUDA;
-    }
     cudaError_t e = cudaSuccess;
     float* base = noalloc_scratch_address(device, &e);
     if (!base) {
@@ -1616,17 +1685,21 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
     Vec<float, 1>* t1 = reinterpret_cast<Vec<float, 1>*>(base);
     Vec<float, 1>* t2 = reinterpret_cast<Vec<float, 1>*>(base + kNoAllocMaxVoxels);
     const float* w = base + 2 * kNoAllocMaxVoxels;
-    noalloc_taps_kernel<<<1, 128, 0, stream>>>(taps);
+    if (launch_on(stream, noalloc_taps_kernel, dim3(1), dim3(128), 0, taps) != cudaSuccess)
+        return IM3D_ERR_CUDA;
     {
         const int S = nh[2] / 2;
         const size_t smem = (size_t)RK * (TK + 2 * S) * sizeof(Vec<float, 1>) + nh[2] * sizeof(float) + 16;
         auto kern = conv_k_kernel<float, 1, TK, RK, LdScalar<float>, StVec<float, 1>>;
         if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
             return IM3D_ERR_CUDA;
+        }
         const long long rows = (long long)nx * ny;
-        kern<<<dim3((unsigned)((rows + RK - 1) / RK), (nz + TK - 1) / TK), dim3(TK, RK), smem, stream>>>(
-            LdScalar<float>{in, d}, StVec<float, 1>{t1, d}, d, w + 2 * NH_MAX, nh[2]);
+        if (launch_on(stream, kern, dim3((unsigned)((rows + RK - 1) / RK), (nz + TK - 1) / TK), dim3(TK, RK),
+                      smem, LdScalar<float>{in, d}, StVec<float, 1>{t1, d}, d, w + 2 * NH_MAX, nh[2]) != cudaSuccess)
+            return IM3D_ERR_CUDA;
     }
     {
         constexpr int TA = TileA<float>::v;
@@ -1634,10 +1707,13 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
         const size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<float, 1>) + nh[1] * sizeof(float) + 16;
         auto kern = conv_s_kernel<float, 1, 1, TW, TY, TA, LdVec<float, 1>, StVec<float, 1>>;
         if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
             return IM3D_ERR_CUDA;
-        kern<<<dim3((nz + TW - 1) / TW, (ny + TA - 1) / TA, nx), dim3(TW, TY), smem, stream>>>(
-            LdVec<float, 1>{t1, d}, StVec<float, 1>{t2, d}, d, w + NH_MAX, nh[1]);
+        }
+        if (launch_on(stream, kern, dim3((nz + TW - 1) / TW, (ny + TA - 1) / TA, nx), dim3(TW, TY), smem,
+                      LdVec<float, 1>{t1, d}, StVec<float, 1>{t2, d}, d, w + NH_MAX, nh[1]) != cudaSuccess)
+            return IM3D_ERR_CUDA;
     }
     {
         constexpr int TA = TileA<float>::v;
@@ -1645,12 +1721,14 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
         const size_t smem = (size_t)(TA + 2 * S) * TW * sizeof(Vec<float, 1>) + nh[0] * sizeof(float) + 16;
         auto kern = conv_s_kernel<float, 1, 0, TW, TY, TA, LdVec<float, 1>, StScalar<float>>;
         if (smem > 48 * 1024 &&
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
             return IM3D_ERR_CUDA;
-        kern<<<dim3((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny), dim3(TW, TY), smem, stream>>>(
-            LdVec<float, 1>{t2, d}, StScalar<float>{out, d}, d, w, nh[0]);
+        }
+        if (launch_on(stream, kern, dim3((nz + TW - 1) / TW, (nx + TA - 1) / TA, ny), dim3(TW, TY), smem,
+                      LdVec<float, 1>{t2, d}, StScalar<float>{out, d}, d, w, nh[0]) != cudaSuccess)
+            return IM3D_ERR_CUDA;
     }
-    if (cudaGetLastError() != cudaSuccess) return IM3D_ERR_CUDA;
     if (cudaStreamSynchronize(stream) != cudaSuccess) {
         cudaGetLastError();
         return IM3D_ERR_CUDA;
@@ -1679,9 +1757,8 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
         im3d_ctx* w = nullptr;
         const int st = im3d_ctx_create(ctx->device, &w);
         if (st != IM3D_OK) return fail(ctx, st, "cannot create a worker context");
-        // the L2 set-aside belongs to the whole CUDA context; concurrent workers would
-        // evict each other's persisting lines, so they stream
-        w->persist_max = 0;
+        w->mem_limit = ctx->mem_limit;
+        w->ifit_chunks = ctx->ifit_chunks;
         ctx->workers.push_back(w);
     }
     std::vector<int> order(nvol);
@@ -1753,6 +1830,11 @@ int enter(im3d_ctx* ctx)
 
 }  // namespace
 
+// ------------------------------------------------- shared with the other units
+cudaStream_t im3d_ctx_stream(im3d_ctx* ctx) { return ctx->stream; }
+int im3d_ctx_device(im3d_ctx* ctx) { return ctx->device; }
+std::string& im3d_ctx_error_ref(im3d_ctx* ctx) { return ctx->err; }
+
 // ====================================================================== C ABI
 extern "C" {
 
@@ -1784,18 +1866,7 @@ int im3d_ctx_create(int device, im3d_ctx** out)
     for (int q = 0; q < 3; ++q) cudaEventCreate(&ctx->ev[q]);
     cudaEventCreateWithFlags(&ctx->ev[3], cudaEventDisableTiming);
     ctx->stream = ctx->own_stream;
-    // L2 pinning of the Gauss-Seidel state is opt-in (IM3D_L2_PERSIST=1): on B200 the
-    // set-aside speeds the half-sweep up (26.9 -> 22.9 us at 256^3) but slows the
-    // streaming kernels of the rest of the iteration more than that
-    const char* tbenv = std::getenv("IM3D_TB");
-    ctx->tb_enabled = tbenv && tbenv[0] == '1';
-    const char* pin = std::getenv("IM3D_L2_PERSIST");
-    ctx->persist_max = (pin && pin[0] == '1' && prop.persistingL2CacheMaxSize > 0)
-                           ? (size_t)prop.persistingL2CacheMaxSize : 0;
-    ctx->window_max = prop.accessPolicyMaxWindowSize > 0 ? (size_t)prop.accessPolicyMaxWindowSize : 0;
     ctx->num_sms = prop.multiProcessorCount;
-    const char* ch = std::getenv("IM3D_IFIT_CHUNKS");
-    ctx->ifit_chunks = ch ? std::atoi(ch) : 0;
     *out = ctx;
     return IM3D_OK;
 }
@@ -1808,11 +1879,6 @@ int im3d_ctx_destroy(im3d_ctx* ctx)
     for (im3d_ctx* w : ctx->workers) im3d_ctx_destroy(w);
     ctx->workers.clear();
     cudaSetDevice(ctx->device);
-    if (ctx->persist_set) {
-        l2_unpin(ctx);
-        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
-        cudaGetLastError();
-    }
     for (auto& kv : ctx->bufs)
         if (kv.second.p) cudaFree(kv.second.p);
     if (ctx->ctrl_d) cudaFree(ctx->ctrl_d);
@@ -1834,6 +1900,63 @@ int im3d_ctx_set_stream(im3d_ctx* ctx, void* stream)
 }
 
 int64_t im3d_ctx_launch_count(const im3d_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    if (value < 0) return fail(ctx, IM3D_ERR_INVALID_ARG, "option values are non negative");
+    switch (option) {
+    case IM3D_OPT_FIT_CHUNKS:
+        ctx->ifit_chunks = value > 0x7fffffff ? 0x7fffffff : (int)value;
+        return IM3D_OK;
+    case IM3D_OPT_DEVICE_MEMORY_LIMIT:
+        ctx->mem_limit = (size_t)value;
+        for (im3d_ctx* w : ctx->workers) w->mem_limit = (size_t)value;
+        return IM3D_OK;
+    default:
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown option " + std::to_string(option));
+    }
+}
+
+int im3d_ctx_set_observer(im3d_ctx* ctx, int every, int with_state, im3d_rsfe_observer cb, void* user)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    if (cb && every <= 0) return fail(ctx, IM3D_ERR_INVALID_ARG, "the observer needs every > 0");
+    ctx->obs = cb;
+    ctx->obs_user = user;
+    ctx->obs_every = cb ? every : 0;
+    ctx->obs_state = with_state ? 1 : 0;
+    return IM3D_OK;
+}
+
+int im3d_ctx_set_warm_start(im3d_ctx* ctx, im3d_unet* net, int mode, double lr)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    if (mode != IM3D_WS_OFF && mode != IM3D_WS_PREDICT && mode != IM3D_WS_TRAIN)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown warm-start mode");
+    if (mode == IM3D_WS_TRAIN && !(lr > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "training needs lr > 0");
+    if (net && im3d::unet::net_device(net) != ctx->device)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "the network lives on another device");
+    ctx->ws_net = mode == IM3D_WS_OFF ? nullptr : net;
+    ctx->ws_mode = net ? mode : IM3D_WS_OFF;
+    ctx->ws_lr = lr;
+    return IM3D_OK;
+}
+
+int im3d_ctx_set_resume(im3d_ctx* ctx, const im3d_rsfe_checkpoint* from, int element_size)
+{
+    if (!ctx) return IM3D_ERR_INVALID_ARG;
+    if (!from) {
+        ctx->resume = false;
+        return IM3D_OK;
+    }
+    if (element_size != 4 && element_size != 8)
+        return fail(ctx, IM3D_ERR_INVALID_ARG, "element_size must be 4 or 8");
+    ctx->resume = true;
+    ctx->resume_from = *from;
+    ctx->resume_esize = element_size;
+    return IM3D_OK;
+}
 
 int im3d_ctx_set_profiling(im3d_ctx* ctx, int on)
 {

@@ -1440,254 +1440,6 @@ __global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
     }
 }
 
-// ---- temporally blocked red-black Gauss-Seidel (two sweeps per pass, FP32) ---------
-// One CTA owns a tile of PJ = TJ + 8 rows by PV = TMV + 2 float4 columns (4 packed
-// cells each) and a chunk [c0, c1) of planes of i; one thread owns one float4 column of
-// the tile and marches it through the planes q = c0-4 .. c1+3. At plane q, level
-// L = 1..4 updates colour (L-1)&1 at plane q-L (red, black, red, black: two full
-// sweeps). A level reads the previous level's values of its own column on planes p-1,
-// p, p+1 from registers, and those of the rows j-1, j+1 and of the next column on the
-// same plane from a shared-memory copy that the previous level stored one plane
-// earlier (double-buffered), so one barrier per plane orders all exchanges. Levels at
-// the tile edge read a zero guard and are wrong there; the wrong values move inward one
-// cell per level, so after four levels the 4-cell halo has absorbed them and the tile
-// interior is exact. The planes of u (both colours) and b_eff stream in through a
-// cp.async ring two planes ahead of use. The update order inside a colour does not
-// matter, so the result is bit-identical to two calls of rb_sweep. The pass is out of
-// place (Uin -> Uout): neighbouring CTAs read overlapping halos of Uin while others
-// write their interiors.
-namespace tbr {
-constexpr int D = 2;        // planes in flight ahead of the one being consumed
-constexpr int NRU = D + 3;  // u ring: planes q-2 .. q+D
-constexpr int NRB = D + 5;  // b_eff ring: planes q-4 .. q+D
-}  // namespace tbr
-
-template <int TJ, int TMV>
-struct TbGeom {
-    static constexpr int PJ = TJ + 8, PV = TMV + 2;  // rows, float4 columns (with halo)
-    static constexpr int NT = PJ * PV;                 // threads: one per float4 column
-    static constexpr int GV = PV + 2;                  // row pitch with a guard each side
-    static constexpr int UPL = (PJ + 2) * GV;          // one guarded plane of one colour
-    static constexpr int BPL = PJ * PV;
-    static constexpr int U_RING = tbr::NRU * 2 * UPL;
-    static constexpr int B_RING = tbr::NRB * 2 * BPL;
-    static constexpr int SLOTS = 3 * 2 * UPL;          // levels 1..3, double-buffered
-    static constexpr size_t SMEM = (size_t)(U_RING + B_RING + SLOTS) * sizeof(float4);
-};
-
-// blockIdx.x = tile (x fastest over packed columns), blockIdx.y = chunk of ci planes.
-template <int TJ, int TMV>
-__global__ void __launch_bounds__(TbGeom<TJ, TMV>::NT, 1)
-    rb_pair_kernel(const float* __restrict__ Uin, float* __restrict__ Uout,
-                   const float* __restrict__ B, Dims d, GsCoef<float> c, int ci)
-{
-    using G = TbGeom<TJ, TMV>;
-    using tbr::D;
-    using tbr::NRB;
-    using tbr::NRU;
-    extern __shared__ __align__(16) float4 tb_sm[];
-    float4* uring = tb_sm;               // [NRU][2][PJ+2][GV]
-    float4* bring = uring + G::U_RING;   // [NRB][2][PJ][PV]
-    float4* slots = bring + G::B_RING;   // [3][2][PJ+2][GV]
-    const int tid = threadIdx.x;
-    const int jl = tid / G::PV, mv = tid - jl * G::PV;
-    const int hz = d.hz();
-    const int gxt = (hz + 4 * TMV - 1) / (4 * TMV);
-    const int bx = blockIdx.x % gxt, by = blockIdx.x / gxt;
-    const int j = by * TJ - 4 + jl;
-    const int mb = bx * 4 * TMV - 4 + 4 * mv;  // packed index of the column's first cell
-    const int c0 = blockIdx.y * ci;
-    const int c1 = min(c0 + ci, d.nx);
-    const int qa = c0 - 4;
-    const int nt = c1 + 4 - qa;
-    const long long plane = (long long)d.ny * hz;
-    const long long npk = plane * d.nx;
-    const bool vin = j >= 0 && j < d.ny && mb >= 0 && mb < hz;  // hz and mb are multiples of 4
-    const long long lofs = vin ? (long long)j * hz + mb : 0;
-    const bool wout = vin && jl >= 4 && jl < 4 + TJ && mv >= 1 && mv <= TMV;
-    const int gown = (jl + 1) * G::GV + mv + 1;
-    const int bown = jl * G::PV + mv;
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int e = tid; e < G::U_RING; e += G::NT) uring[e] = z4;
-    for (int e = tid; e < G::SLOTS; e += G::NT) slots[e] = z4;
-    __syncthreads();
-
-    auto issue = [&](int t) {
-        if (t < nt) {
-            const int q = qa + t;
-            float4* u0 = uring + (t % NRU) * 2 * G::UPL + gown;
-            float4* b0 = bring + (t % NRB) * 2 * G::BPL + bown;
-            if (vin && q >= 0 && q < d.nx) {
-                const long long g = (long long)q * plane + lofs;
-                cp_async16(u0, Uin + g);
-                cp_async16(u0 + G::UPL, Uin + npk + g);
-                cp_async16(b0, B + g);
-                cp_async16(b0 + G::BPL, B + npk + g);
-            } else {
-                u0[0] = z4;
-                u0[G::UPL] = z4;
-                b0[0] = z4;
-                b0[G::BPL] = z4;
-            }
-        }
-        cp_async_commit();
-    };
-
-    const bool jint = j >= 1 && j <= d.ny - 2;
-    const int cy = j == 0 ? 0 : (j == d.ny - 1 ? 2 : 1);
-    const float hxf = (float)c.hx, hyf = (float)c.hy, hzf = (float)c.hz;
-    // interior cells of this column for the two parities (bit e: cell e has
-    // 1 <= k <= nz-2); with Dirichlet conditions exactly the cells a level updates
-    unsigned kin[2] = {0u, 0u};
-#pragma unroll
-    for (int pr = 0; pr < 2; ++pr)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int k = 2 * (mb + e) + pr;
-            if (vin && jint && k >= 1 && k <= d.nz - 2) kin[pr] |= 1u << e;
-        }
-    const unsigned kin0 = kin[0], kin1 = kin[1];
-    // Neumann: this column holds a cell on a j or k face (or lies in the padding)
-    const bool nedge = c.neu && vin && (!jint || kin0 != 15u || kin1 != 15u);
-    // One level on this thread's column at plane p. xm/ctr/xp: the other colour on planes
-    // p-1, p, p+1 (previous level); ym/yp: rows j-1, j+1 and kn: the neighbouring cell in
-    // the next column (k-1 for par 0, k+1 for par 1) of that colour on plane p; old: this
-    // colour's current value; b: b_eff of this colour. Interior cells use the rb_half formula. Dirichlet boundary and padding cells keep
-    // their value (selects, no branch). Neumann boundary cells take gs_value's float
-    // arithmetic (ghost value -bcn*h for the missing neighbour, same roundings) in a
-    // branch that only columns holding such cells enter.
-    auto level = [&](int p, int par, const float4 xm, const float4 ctr, const float4 xp,
-                     const float4 ym, const float4 yp, const float kn, const float4 old,
-                     const float4 b) -> float4 {
-        const float xmv[4] = {xm.x, xm.y, xm.z, xm.w};
-        const float xpv[4] = {xp.x, xp.y, xp.z, xp.w};
-        const float cv[4] = {ctr.x, ctr.y, ctr.z, ctr.w};
-        const float ymv[4] = {ym.x, ym.y, ym.z, ym.w};
-        const float ypv[4] = {yp.x, yp.y, yp.z, yp.w};
-        const float bv[4] = {b.x, b.y, b.z, b.w};
-        const float ov[4] = {old.x, old.y, old.z, old.w};
-        const unsigned m = (p >= 1 && p <= d.nx - 2) ? (par ? kin1 : kin0) : 0u;
-        float f[4], zo[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            zo[e] = par ? (e < 3 ? cv[e + 1] : kn) : (e > 0 ? cv[e - 1] : kn);
-            const float sx = xmv[e] + xpv[e];
-            const float sy = ymv[e] + ypv[e];
-            const float sz = cv[e] + zo[e];
-            const float v = fmaf(sx, c.ihx2, fmaf(sy, c.ihy2, fmaf(sz, c.ihz2, bv[e]))) * c.htilde[7];
-            f[e] = (m >> e) & 1u ? v : ov[e];
-        }
-        if (c.neu && vin && (nedge || p == 0 || p == d.nx - 1)) {
-            const int cx = p == 0 ? 0 : (p == d.nx - 1 ? 2 : 1);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int k = 2 * (mb + e) + par;
-                if (((m >> e) & 1u) || k >= d.nz) continue;
-                const int cz = k == 0 ? 0 : (k == d.nz - 1 ? 2 : 1);
-                const int nbd = (cx != 1) + (cy != 1) + (cz != 1);
-                const float bcn = nbd == 0 ? c.bcn[0] : nbd == 1 ? c.bcn[1] : nbd == 2 ? c.bcn[2] : c.bcn[3];
-                const int hi = (cx == 1) | ((cy == 1) << 1) | ((cz == 1) << 2);
-                float ht = c.htilde[0];
-                ht = hi == 1 ? c.htilde[1] : ht;
-                ht = hi == 2 ? c.htilde[2] : ht;
-                ht = hi == 3 ? c.htilde[3] : ht;
-                ht = hi == 4 ? c.htilde[4] : ht;
-                ht = hi == 5 ? c.htilde[5] : ht;
-                ht = hi == 6 ? c.htilde[6] : ht;
-                ht = hi == 7 ? c.htilde[7] : ht;
-                const float zp = par ? zo[e] : cv[e];
-                const float zm = par ? cv[e] : zo[e];
-                const float gx = bcn * hxf, gy = bcn * hyf, gz = bcn * hzf;
-                const float tx = (cx == 1 ? xpv[e] + xmv[e] : (cx == 0 ? xpv[e] - gx : xmv[e] + gx)) * c.ihx2;
-                const float ty = (cy == 1 ? ypv[e] + ymv[e] : (cy == 0 ? ypv[e] - gy : ymv[e] + gy)) * c.ihy2;
-                const float tz = (cz == 1 ? zp + zm : (cz == 0 ? zp - gz : zm + gz)) * c.ihz2;
-                const float acc = tx + ty + tz + bv[e];
-                f[e] = acc * ht;
-            }
-        }
-        return make_float4(f[0], f[1], f[2], f[3]);
-    };
-
-    float4 h1[3], h2[3], h3[3], h4 = z4;  // level outputs of the last three plane steps
-#pragma unroll
-    for (int r = 0; r < 3; ++r) h1[r] = h2[r] = h3[r] = z4;
-    for (int t = 0; t < D; ++t) issue(t);
-    // ring slots of plane steps t, t-1, t-2 (u) and t-1 .. t-4 (b_eff), advanced per step
-    int iu0 = 0, iu1 = NRU - 1, iu2 = NRU - 2;
-    int ib1 = NRB - 1, ib2 = NRB - 2, ib3 = NRB - 3, ib4 = NRB - 4;
-
-    auto step = [&](auto Rc, int t) {
-        constexpr int R = decltype(Rc)::value;  // t % 3: h*[R] is this step's output
-        constexpr int R1 = (R + 2) % 3;         // step t-1
-        constexpr int R2 = (R + 1) % 3;         // step t-2
-        if (t >= nt) return;
-        cp_async_wait<D - 1>();
-        __syncthreads();
-        issue(t + D);
-        const int q = qa + t;
-        const int sb = t & 1;
-        // every level of this step updates cells of the same parity (p + j + colour)
-        const int par = (q + j + 1) & 1;
-        const int kno = par ? 4 * (gown + 1) : 4 * (gown - 1) + 3;  // float offset of kn
-        const float4* u_t0 = uring + iu0 * 2 * G::UPL;  // plane q
-        const float4* u_t1 = uring + iu1 * 2 * G::UPL;  // plane q-1
-        const float4* u_t2 = uring + iu2 * 2 * G::UPL;  // plane q-2
-        float4* ws = slots + sb * G::UPL;               // level L writes ws + 2(L-1)*UPL
-        const float4* rs = slots + (sb ^ 1) * G::UPL;   // level L+1 reads rs + 2(L-1)*UPL
-        auto nbr = [&](const float4* pl, float4& ym, float4& yp) -> float {
-            ym = pl[gown - G::GV];
-            yp = pl[gown + G::GV];
-            return reinterpret_cast<const float*>(pl)[kno];
-        };
-        float4 ym, yp;
-        int p = q - 1;  // level 1: colour 0, from the loaded colour 1
-        if (t >= 2 && p >= 0 && p < d.nx) {
-            const float4* n1 = u_t1 + G::UPL;
-            const float kn = nbr(n1, ym, yp);
-            h1[R] = level(p, par, u_t2[G::UPL + gown], n1[gown], u_t0[G::UPL + gown], ym, yp, kn,
-                          u_t1[gown], bring[(ib1 * 2 + 0) * G::BPL + bown]);
-            ws[gown] = h1[R];
-        }
-        p = q - 2;  // level 2: colour 1
-        if (t >= 4 && p >= 0 && p < d.nx) {
-            const float kn = nbr(rs, ym, yp);
-            h2[R] = level(p, par, h1[R2], h1[R1], h1[R], ym, yp, kn, u_t2[G::UPL + gown],
-                          bring[(ib2 * 2 + 1) * G::BPL + bown]);
-            ws[2 * G::UPL + gown] = h2[R];
-        }
-        p = q - 3;  // level 3: colour 0
-        if (t >= 6 && p >= 0 && p < d.nx) {
-            const float kn = nbr(rs + 2 * G::UPL, ym, yp);
-            h3[R] = level(p, par, h2[R2], h2[R1], h2[R], ym, yp, kn, h1[R2],
-                          bring[(ib3 * 2 + 0) * G::BPL + bown]);
-            ws[4 * G::UPL + gown] = h3[R];
-        }
-        p = q - 4;  // level 4: colour 1; plane q-4 is then final
-        if (t >= 8 && p >= 0 && p < d.nx) {
-            const float kn = nbr(rs + 4 * G::UPL, ym, yp);
-            h4 = level(p, par, h3[R2], h3[R1], h3[R], ym, yp, kn, h2[R2],
-                       bring[(ib4 * 2 + 1) * G::BPL + bown]);
-            if (wout && p < c1) {
-                const long long g = (long long)p * plane + lofs;
-                *reinterpret_cast<float4*>(Uout + g) = h3[R1];
-                *reinterpret_cast<float4*>(Uout + npk + g) = h4;
-            }
-        }
-        iu2 = iu1;
-        iu1 = iu0;
-        iu0 = iu0 + 1 == NRU ? 0 : iu0 + 1;
-        ib4 = ib3;
-        ib3 = ib2;
-        ib2 = ib1;
-        ib1 = ib1 + 1 == NRB ? 0 : ib1 + 1;
-    };
-    for (int t = 0; t < nt; t += 3) {
-        step(std::integral_constant<int, 0>(), t);
-        step(std::integral_constant<int, 1>(), t + 1);
-        step(std::integral_constant<int, 2>(), t + 2);
-    }
-}
-
 // ---- vectorised natural-layout kernels (nz a multiple of W = 16/sizeof(T)) ----
 // Thread per group of W consecutive k of row j, marching over NI planes of i.
 
@@ -1994,13 +1746,16 @@ template <typename T>
 __global__ void minmax_kernel(const T* __restrict__ p, long long n, unsigned long long* umax)
 {
     unsigned long long mx = 0, mn = 0;
+    bool bad = false;  // a NaN or Inf seen: umax[3] is raised
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
          q += (long long)gridDim.x * blockDim.x) {
         const double v = (double)p[q];
+        bad |= !isfinite(v);
         const unsigned long long a = order_key(v), b = order_key(-v);
         mx = a > mx ? a : mx;
         mn = b > mn ? b : mn;
     }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicMax(umax + 3, 1ull);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long a = __shfl_xor_sync(0xffffffffu, mx, o);
@@ -2151,6 +1906,54 @@ __global__ void cube_kernel(T* p, Dims d, int ix, int iy, int iz, int fx, int fy
     if (k >= d.nz || j >= d.ny) return;
     const bool in = i >= ix && i < fx && j >= iy && j < fy && k >= iz && k < fz;
     p[d.idx(i, j, k)] = in ? b0 : a0;
+}
+
+// ---- learned warm start: fields of one Poisson solve to and from the network ----
+// Packed cell of natural (i, j, k): its colour's array at d.pidx(i, j, k).
+__device__ __forceinline__ long long packed_at(const Dims& d, int i, int j, int k)
+{
+    return d.pidx(i, j, k) + (((i + j + k) & 1) ? d.npk() : 0);
+}
+
+// The network's inputs, four FP32 volumes x[f][n] (natural layout): the forcing term
+// rhs = b_eff - u_in / dt, the previous solve's u, div(d - b) and phi.
+__global__ void ws_fields_kernel(const float* __restrict__ bpk, const float* __restrict__ upk,
+                                 const float* __restrict__ prevu, const float* __restrict__ divdb,
+                                 const float* __restrict__ phi, Dims d, float inv_dt, float* __restrict__ x)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return;
+    const long long v = d.idx(i, j, k), pv = packed_at(d, i, j, k), n = d.n();
+    x[v] = bpk[pv] - upk[pv] * inv_dt;
+    x[n + v] = prevu[v];
+    x[2 * n + v] = divdb[v];
+    x[3 * n + v] = phi[v];
+}
+
+// u_in += the network's correction y on the cells the solve updates (all cells with
+// Neumann conditions, the interior with Dirichlet ones, whose faces keep their value).
+__global__ void ws_apply_kernel(float* __restrict__ upk, const float* __restrict__ y, Dims d, int dirichlet)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return;
+    if (dirichlet && (i == 0 || j == 0 || k == 0 || i == d.nx - 1 || j == d.ny - 1 || k == d.nz - 1)) return;
+    upk[packed_at(d, i, j, k)] += y[d.idx(i, j, k)];
+}
+
+// The correction the solve made, natural layout: t = u_solved - u_in.
+__global__ void ws_target_kernel(const float* __restrict__ upk, const float* __restrict__ upk0, Dims d,
+                                 float* __restrict__ t)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return;
+    const long long pv = packed_at(d, i, j, k);
+    t[d.idx(i, j, k)] = upk[pv] - upk0[pv];
 }
 
 }  // namespace im3d

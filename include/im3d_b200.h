@@ -36,6 +36,9 @@ extern "C" {
 #define IM3D_ERR_OOM 5           /* device allocation failed */
 #define IM3D_ERR_NO_DEVICE 6     /* no usable sm_100 device */
 #define IM3D_ERR_TOO_LARGE 7     /* volume above the fixed scratch of a no-allocation entry point */
+#define IM3D_ERR_NONFINITE 8     /* an input volume holds NaN or Inf (the reference's debug build
+                                    traps such values as floating-point exceptions,
+                                    exceptions.hxx:25-35; here the call refuses them) */
 
 /* Boundary condition selector. The reference keeps bc_type private
  * (rsfe_splitbregman.hxx:108); its constructor sets bc = NEU but installs
@@ -117,6 +120,9 @@ typedef struct im3d_rsfe_stats {
     int32_t last_sweeps;  /* sweeps of the last outer iteration */
     int32_t not_converged;/* outer iterations whose solve hit gs_max_sweeps */
     int32_t residual_checks; /* residual evaluations of the Poisson solves (residual mode) */
+    int32_t ws_used;      /* solves started from the learned warm start (IM3D_WS_PREDICT) */
+    int32_t ws_rejected;  /* solves where it lost to the previous iterate */
+    double ws_loss;       /* mean training loss over the solves (IM3D_WS_TRAIN) */
 } im3d_rsfe_stats;
 
 typedef struct im3d_ctx im3d_ctx;
@@ -129,6 +135,19 @@ const char* im3d_ctx_last_error(const im3d_ctx* ctx);
 int im3d_ctx_set_stream(im3d_ctx* ctx, void* cuda_stream);
 /* Count of kernel launches the context issued since creation (instrumentation). */
 int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
+
+/* Context options (no counterpart in the reference), set with im3d_ctx_set_option:
+ *  IM3D_OPT_FIT_CHUNKS           chunks of planes along i of the FP32 fitting stage;
+ *                                0 (default) = the cost model's choice. Every choice
+ *                                gives bit-identical results.
+ *  IM3D_OPT_DEVICE_MEMORY_LIMIT  bytes of device buffers the context may hold; a call
+ *                                that would need more returns IM3D_ERR_OOM before it
+ *                                allocates (0, the default, = no limit). For callers that
+ *                                share the GPU under a memory budget.
+ * Returns IM3D_ERR_INVALID_ARG for an unknown option or a negative value. */
+#define IM3D_OPT_FIT_CHUNKS 1
+#define IM3D_OPT_DEVICE_MEMORY_LIMIT 2
+int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value);
 /* Per-stage device timing: with profiling on, each launch of the loop's kernels is
  * bracketed by CUDA events on the launching stream. im3d_ctx_profile() synchronises,
  * writes up to max_entries stage names ('\n'-separated into names), total ms and
@@ -195,16 +214,18 @@ int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, in
  * second allocator must not fragment), code inside a hard device-memory budget, and
  * code that must not make the allocation calls that can synchronise the device. The
  * caller passes device buffers `in` and `out` (nx*ny*nz floats each, on the current
- * device) and a cudaStream_t (NULL = the default stream); the call returns after the
- * filter has finished on that stream. It is im3d_gauss_filter_f32 with its two
- * intermediate volumes and its taps held in one file-scope __device__ array of
- * 2 * 2097152 + 387 floats (16 MiB), which every GPU that loads the library keeps
- * until the process exits. Volumes above 2097152 voxels (128^3) return
- * IM3D_ERR_TOO_LARGE without touching the GPU. The first call on a device looks the
- * array's device address up (cudaGetSymbolAddress); make that first call before any
- * stream capture. Calls share the array, so calls that overlap on the GPU (other
- * threads or streams) race; every call rewrites all of the scratch it reads, so
- * nothing carries over from the previous call. */
+ * device; pointers of another device return IM3D_ERR_INVALID_ARG) and a cudaStream_t
+ * (NULL = the default stream); every call waits for that stream to finish before it
+ * returns. It is im3d_gauss_filter_f32 with its two intermediate volumes and its taps
+ * held in one file-scope __device__ array of 2 * 2097152 + 387 floats (16 MiB), which
+ * every GPU that loads the library keeps until the process exits. Volumes above
+ * 2097152 voxels (128^3) return IM3D_ERR_TOO_LARGE, and nx or ny above 65535 return
+ * IM3D_ERR_INVALID_ARG, both without touching the GPU. The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture. Calls share the array, so calls that overlap on the GPU
+ * (other threads or streams) race; every call rewrites all of the scratch it reads,
+ * so nothing carries over from the previous call. A launch that fails returns
+ * IM3D_ERR_CUDA; an error the caller left pending is neither reported nor cleared. */
 int im3d_gauss_filter_f32_noalloc(const float* in, float* out, int nx, int ny, int nz,
                                   double hx, double hy, double hz, double sigma, double radius,
                                   int pixel_approach, void* stream);
@@ -224,7 +245,8 @@ int im3d_div_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, i
  * init == NULL is apply(myim) with the default cube (:1531-1543, :48-95).
  * phi_out receives getoutput() (segmentation.hxx:108-111). u_out (phi after the last
  * solve, before the clamp), f1_out and f2_out (the last iteration's fitting means,
- * :1709-1717) are optional (NULL = not copied). */
+ * :1709-1717) are optional (NULL = not copied). A myim or init holding NaN or Inf
+ * returns IM3D_ERR_NONFINITE before the loop starts. */
 int im3d_rsfe_apply_f32(im3d_ctx* ctx, const float* myim, const float* init, int nx, int ny,
                         int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
                         float* phi_out, float* u_out, float* f1_out, float* f2_out,
@@ -233,6 +255,99 @@ int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, i
                         int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
                         double* phi_out, double* u_out, double* f1_out, double* f2_out,
                         im3d_rsfe_stats* stats);
+
+/* State of the loop after outer iteration t: what rsfe_splitbregman<T> holds between
+ * iterations (phi, the Bregman variable b and div(d - b)), plus this backend's
+ * residual-schedule state, so that a run resumed from it continues exactly as the
+ * uninterrupted run would. Arrays are T (float for _f32, double for _f64) in the
+ * image3d layout; b holds 3 volumes, component-major. */
+typedef struct im3d_rsfe_checkpoint {
+    int32_t t;               /* outer iterations completed */
+    int32_t init_variables;  /* the next iteration resets b and div(d-b) (after an extraction) */
+    int32_t sched_first;     /* sweeps before the first residual check of the next solve */
+    int32_t reserved;
+    double sched_rate;       /* contraction rate carried to the next solve */
+    double tollerance;       /* ||phi - phiold||_L2 / ||phiold||_L2 of iteration t */
+    void* phi;               /* n values */
+    void* b;                 /* 3n values (NULL when the observer did not ask for the state) */
+    void* divdb;             /* n values (NULL likewise) */
+} im3d_rsfe_checkpoint;
+
+/* Per-iteration observer of im3d_rsfe_apply_*: the dumps of the reference's loop
+ * (dumpfrequency, rsfe_splitbregman_imp.hxx:1940-1951, which writes phi every
+ * dumpfrequency-th iteration except the last) and full-state checkpoints. After
+ * outer iteration t, when every > 0, t % every == 0 and t != maxiter, the loop copies
+ * phi (and with with_state != 0 also b and div(d-b)) to host memory owned by the
+ * context and calls cb(user, &checkpoint); the pointers are valid during the call
+ * only. A non-zero return ends the loop after that iteration, as the reference's
+ * end_now does (:1659). cb == NULL removes the observer. The other iterations copy
+ * nothing. No counterpart as a function in the reference. */
+typedef int (*im3d_rsfe_observer)(void* user, const im3d_rsfe_checkpoint* state);
+int im3d_ctx_set_observer(im3d_ctx* ctx, int every, int with_state, im3d_rsfe_observer cb,
+                          void* user);
+
+/* Resume: the next im3d_rsfe_apply_* call on this context starts from `from` instead
+ * of the initial level set (its init argument is then ignored), at outer iteration
+ * from->t + 1, with the set-up (filters, edge detector) recomputed from myim. phi, b
+ * and divdb must be set (host or device memory holding values of element_size bytes:
+ * 4 for the _f32 call, 8 for _f64) and stay valid until that call returns; the
+ * struct itself is copied here. The result equals the uninterrupted run's bit for bit.
+ * from == NULL cancels a pending resume. The reference can only restart from phi
+ * (apply(myim, init) rescales init and zeroes b, :99-170, :1606-1629). */
+int im3d_ctx_set_resume(im3d_ctx* ctx, const im3d_rsfe_checkpoint* from, int element_size);
+
+/* ---- Learned warm start of the Poisson step (no counterpart in the reference) ----
+ * A 3-level 3-D U-Net (16/32/64 channels, 3x3x3 convolutions, ReLU, 2x2x2 max pooling
+ * and transposed convolutions, a 1x1 output layer) maps four fields of an outer
+ * iteration -- the forcing term rhs, the previous solve's u, div(d - b) and phi -- to a
+ * correction of phi that starts the Gauss-Seidel solve of
+ * rsfe_splitbregman_imp.hxx:1768-1785 (poisson_imp.hxx:340-429). Activations are BF16
+ * (channels last), filters BF16 with FP32 master copies, accumulation FP32 on the
+ * tensor cores (tcgen05). The solve still runs to the requested residual after it. */
+typedef struct im3d_unet im3d_unet;
+
+/* A network with He-normal weights from `seed` (the output layer starts at zero, so an
+ * untrained network predicts no correction), on the context's device. */
+int im3d_unet_create(im3d_ctx* ctx, uint64_t seed, im3d_unet** out);
+int im3d_unet_destroy(im3d_unet* net);
+/* Parameters as FP32, in this order per 3x3x3 layer (e1a, e1b, e2a, e2b, e3a, e3b,
+ * d2a, d2b, d1a, d1b): W[cout][cin][27] (tap = 9 dz + 3 dy + dx over the (i, j, k)
+ * offsets -1..1), bias[cout]; then the transposed convolutions up2 (64 -> 32) and up1
+ * (32 -> 16): U[8][cin][cout] (child o = 4 di + 2 dj + dk), bias[cout]; then the 1x1
+ * output layer: w[16], bias[1]. */
+int64_t im3d_unet_param_count(const im3d_unet* net);
+int im3d_unet_get_params(im3d_ctx* ctx, im3d_unet* net, float* host, int64_t count);
+int im3d_unet_set_params(im3d_ctx* ctx, im3d_unet* net, const float* host, int64_t count);
+/* Forward pass of nsamp samples: x holds nsamp x 4 FP32 volumes [s][field][nx][ny][nz]
+ * (host or device), y receives nsamp FP32 volumes. nx, ny: multiples of 4; nz, nz/2,
+ * nz/4 multiples of 16 that are at most 128 or multiples of 128. */
+int im3d_unet_forward(im3d_ctx* ctx, im3d_unet* net, const float* x, int nsamp, int nx, int ny, int nz,
+                      float* y);
+/* One training step on (x, target): forward, mean squared error, backward (BF16
+ * tensor-core data and weight gradients), Adam with learning rate lr (lr = 0: no
+ * update). *loss (may be NULL) receives the loss of the forward pass, grads (host, may
+ * be NULL) the FP32 gradient of every parameter in the order above. */
+int im3d_unet_train_step(im3d_ctx* ctx, im3d_unet* net, const float* x, const float* target, int nsamp, int nx,
+                         int ny, int nz, double lr, double* loss, float* grads);
+/* One 3x3x3 convolution (zero padding, stride 1) on the tensor cores, as the network's
+ * layers run it: x BF16 channels-last (c_pitch channels per voxel, the cin used ones
+ * from c_off), w FP32 [cout][cin][27], bias FP32 [cout] or NULL, out FP32 channels-last
+ * [voxel][cout]; cin, cout in {16, 32, 64}; all pointers device memory. */
+int im3d_conv3d_bf16(im3d_ctx* ctx, const uint16_t* x, int c_pitch, int c_off, int cin, const float* w,
+                     const float* bias, int cout, int nsamp, int nx, int ny, int nz, float* out);
+
+/* The warm start inside im3d_rsfe_apply_f32 when gs_rel_res_tol > 0:
+ *  IM3D_WS_PREDICT  before each solve the network's correction is added to phi; the
+ *                   solve starts from it when its residual is below the previous
+ *                   iterate's, and from the previous iterate otherwise;
+ *  IM3D_WS_TRAIN    after each solve the network takes one training step (learning
+ *                   rate lr) on that solve's fields and its solution (the pairs the
+ *                   plain solver generates); the solve itself is the plain one.
+ * net == NULL or mode IM3D_WS_OFF removes it. The network must stay alive while set. */
+#define IM3D_WS_OFF 0
+#define IM3D_WS_PREDICT 1
+#define IM3D_WS_TRAIN 2
+int im3d_ctx_set_warm_start(im3d_ctx* ctx, im3d_unet* net, int mode, double lr);
 
 /* Connected component of the thresholded image, as
  * image3d<T>::connected_component (image3d_imp.hxx:1694-2120):

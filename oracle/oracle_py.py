@@ -54,7 +54,8 @@ class RsfeStats(C.Structure):
         ("last_tol", C.c_double), ("last_rel_res", C.c_double), ("last_ls_err", C.c_double),
         ("setup_ms", C.c_double), ("loop_ms", C.c_double), ("total_sweeps", C.c_int64),
         ("iterations", C.c_int32), ("last_sweeps", C.c_int32), ("not_converged", C.c_int32),
-        ("residual_checks", C.c_int32),
+        ("residual_checks", C.c_int32), ("ws_used", C.c_int32), ("ws_rejected", C.c_int32),
+        ("ws_loss", C.c_double),
     ]
 
 

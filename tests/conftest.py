@@ -17,9 +17,12 @@ def pytest_configure(config):
     # the CPU checker is test infrastructure; build it if a fresh checkout lacks it
     if not os.path.exists(os.path.join(ORACLE, "liboracle.so")):
         subprocess.call(["make", "-s", "-C", ORACLE, "liboracle.so"])
+    import __graft_entry__
+
+    ref = __graft_entry__.REFERENCE
     if (not os.path.exists(os.path.join(ORACLE, "_ref", "libim3d_ref.so"))
-            and os.path.isdir("/root/reference/header")):
-        subprocess.call(["make", "-s", "-C", ORACLE, "ref"])
+            and os.path.isdir(os.path.join(ref, "header"))):
+        subprocess.call(["make", "-s", "-C", ORACLE, "ref", f"REF={ref}"])
 
 
 @pytest.fixture(scope="session")

@@ -114,17 +114,17 @@ def test_fp32_fit_stage_shapes(ctx, pkg, O, shape, extra):
     assert pkg.synth.dice(got["phi"], want["phi"]) >= 0.999
 
 
-def test_fp32_fit_stage_chunking_bit_identical(pkg, monkeypatch):
+def test_fp32_fit_stage_chunking_bit_identical(pkg):
     """The i-axis march gives every output cell the same operations whatever the chunk
     count, so the results are bit-identical for 1, 3 and 7 chunks and the cost model's
-    choice."""
+    choice (context option IM3D_OPT_FIT_CHUNKS)."""
     u0, phi0 = _case(pkg, (75, 34, 40), seed=9, r=12.0)
     params = pkg.default_params(**{**BASE, "maxiter": 3, "bc": 2})
     outs = []
-    for chunks in ("1", "3", "7", "0"):
-        monkeypatch.setenv("IM3D_IFIT_CHUNKS", chunks)
+    for chunks in (1, 3, 7, 0):
         c = pkg.Context(0)
         try:
+            c.set_option(pkg.OPT_FIT_CHUNKS, chunks)
             outs.append(c.rsfe_apply(u0.astype(np.float32), phi0.astype(np.float32), params,
                                      want_u=True, want_f=True))
         finally:

@@ -6,10 +6,12 @@ code that must not make allocation calls that can synchronise the device). It ke
 its intermediate volumes in a fixed __device__ array instead of context buffers.
 This test calls it through the C ABI twice in a row, on two different volumes, and
 checks each result against the allocating entry point im3d_gauss_filter_f32, with
-the FP32 tolerance the other filter tests use. It also checks that a volume above
-the fixed capacity is refused before anything runs. It sits in its own file named
-to be collected last, and builds everything it needs itself, so it passes alone in
-a fresh process as well as after the other tests.
+the FP32 tolerance the other filter tests use; then on a stream the caller owns, with
+inputs written on that stream, and on a small odd volume whose axes are shorter than
+the Gaussian's support. It also checks that a volume above the fixed capacity, and
+one whose launch geometry does not fit, are refused before anything runs. It sits in
+its own file named to be collected last, and builds everything it needs itself, so
+it passes alone in a fresh process as well as after the other tests.
 """
 import ctypes as C
 import importlib
@@ -58,3 +60,33 @@ def test_noalloc_filter_refuses_volumes_above_its_scratch():
     assert x.numel() > MAX_VOXELS
     out = torch.empty_like(x)
     assert _noalloc(pkg.lib(), x, out, 2.0, (1.0, 1.0, 1.0)) == 7
+
+
+def test_noalloc_filter_on_a_caller_stream_and_a_small_odd_volume():
+    torch = pytest.importorskip("torch")
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    lib = pkg.lib()
+    stream = torch.cuda.Stream()
+    with pkg.Context(0) as ctx:
+        for shape, sigma in (((96, 80, 72), 3.0), ((7, 9, 11), 2.0)):
+            with torch.cuda.stream(stream):
+                g = torch.Generator(device="cuda")
+                g.manual_seed(7)
+                x = torch.rand(shape, device="cuda", generator=g)
+                out = torch.full_like(x, float("nan"))
+            st = _noalloc(lib, x, out, sigma, (1.0, 1.0, 1.0), stream=stream.cuda_stream)
+            assert st == 0, st
+            got = out.cpu().numpy()  # the call returned after its stream finished
+            want = ctx.gauss_filter(x.cpu().numpy(), sigma)
+            assert np.isfinite(got).all()
+            assert _rel(got, want) < 2e-6, shape
+
+
+def test_noalloc_filter_refuses_a_launch_geometry_that_does_not_fit():
+    torch = pytest.importorskip("torch")
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    x = torch.zeros((70000, 3, 3), dtype=torch.float32, device="cuda")
+    assert x.numel() <= MAX_VOXELS
+    out = torch.full_like(x, 5.0)
+    assert _noalloc(pkg.lib(), x, out, 1.0, (1.0, 1.0, 1.0)) == 1
+    assert bool((out == 5.0).all())  # nothing was written
