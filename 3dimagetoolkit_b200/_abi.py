@@ -221,7 +221,8 @@ class Context:
             raise Im3dError(st, self.last_error())
         return st
 
-    def set_profiling(self, on: bool = True):
+    def set_profiling(self, on: int = 1):
+        """1 (True): every stage; 2: the Poisson solves as a whole only; 0: off."""
         self._check(lib().im3d_ctx_set_profiling(self._h, C.c_int(int(on))))
 
     def profile(self, reset: bool = True) -> dict:

@@ -185,7 +185,7 @@ __device__ __forceinline__ void block_sum2_store(double a, double b, double* par
 // four interleaved accumulators (m mod 4), so that four loads are in flight, then the
 // block adds the accumulators and the threads' sums in a fixed tree.
 constexpr int kFinThreads = 1024;
-__global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const double* __restrict__ part,
+static __global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const double* __restrict__ part,
                                                                     long long nblocks, int nvals,
                                                                     double* sums, int slot)
 {

@@ -25,6 +25,14 @@
 
 using namespace im3d;
 
+// The library is built from this file twice: unit 1 (compiled with -fmad=false, so that
+// the FP64 path keeps the reference's operations bit for bit) holds the context, the
+// generic entry points and the _f64 ones; unit 2 (im3d_b200_f32.cu, compiled with
+// contracted multiply-adds) holds the _f32 entry points. 0 builds everything.
+#ifndef IM3D_UNIT
+#define IM3D_UNIT 0
+#endif
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -42,7 +50,7 @@ struct im3d_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // [3]: tolerance copy done
     // per-stage device timing (im3d_ctx_set_profiling): events recorded on the
     // launching stream around each launch, resolved at the next synchronisation
-    bool prof = false;
+    int prof = 0;  // 1: every stage; 2: the Poisson solves as a whole only
     std::vector<cudaEvent_t> ev_pool;
     struct Pending {
         std::string name;
@@ -127,6 +135,7 @@ cudaEvent_t prof_event(im3d_ctx* ctx)
 int prof_begin(im3d_ctx* ctx, const char* name)
 {
     if (!ctx->prof) return -1;
+    if (ctx->prof == 2 && std::strcmp(name, "poisson_solve") != 0) return -1;
     im3d_ctx::Pending pd{name, prof_event(ctx), prof_event(ctx)};
     cudaEventRecord(pd.a, ctx->stream);
     ctx->pending.push_back(pd);
@@ -1224,6 +1233,9 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             // check after as many sweeps as it needed, its contraction rate as the first
             // prediction (the sweep counts of consecutive solves differ by a sweep or two)
             double rate = 0;
+            // the whole solve, warm start included, as one more profiled stage (it
+            // encloses the half-sweep and residual stages): the time to tolerance
+            const int pfs = prof_begin(ctx, "poisson_solve");
             if constexpr (std::is_same<T, float>::value) {
                 if (ws)
                     IM3D_TRY(ws_before(ctx, d, coef, upk, bpk, u_d, divdb, phi, (float)(1.0 / p->dt), neu ? 0 : 1,
@@ -1232,6 +1244,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             IM3D_TRY(rb_solve<T>(ctx, upk, bpk, d, coef, p->gs_rel_res_tol, p->gs_max_sweeps,
                                  p->gs_check_every, p->omega, &sw, &rel, &conv, sched_first,
                                  sched_rate, &rate));
+            prof_end(ctx, pfs);
             if constexpr (std::is_same<T, float>::value) {
                 if (ws && ctx->ws_mode == IM3D_WS_TRAIN) {
                     double l = 0;
@@ -1570,6 +1583,7 @@ int poisson_solve(im3d_ctx* ctx, T* u_user, const T* b_user, int nx, int ny, int
     return IM3D_OK;
 }
 
+#if IM3D_UNIT != 1
 // ------------------------------------------------ Gaussian filter, no allocation
 // Fixed scratch of im3d_gauss_filter_f32_noalloc: two intermediate volumes of up to
 // kNoAllocMaxVoxels voxels, then the three axes' taps.
@@ -1736,6 +1750,8 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
     return IM3D_OK;
 }
 
+#endif  // IM3D_UNIT != 1
+
 template <typename T>
 int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, int ny, int nz,
                double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
@@ -1830,14 +1846,18 @@ int enter(im3d_ctx* ctx)
 
 }  // namespace
 
+#if IM3D_UNIT != 2
 // ------------------------------------------------- shared with the other units
 cudaStream_t im3d_ctx_stream(im3d_ctx* ctx) { return ctx->stream; }
 int im3d_ctx_device(im3d_ctx* ctx) { return ctx->device; }
 std::string& im3d_ctx_error_ref(im3d_ctx* ctx) { return ctx->err; }
 
 // ====================================================================== C ABI
+#endif
+
 extern "C" {
 
+#if IM3D_UNIT != 2
 int im3d_ctx_create(int device, im3d_ctx** out)
 {
     if (!out) return IM3D_ERR_INVALID_ARG;
@@ -1961,7 +1981,7 @@ int im3d_ctx_set_resume(im3d_ctx* ctx, const im3d_rsfe_checkpoint* from, int ele
 int im3d_ctx_set_profiling(im3d_ctx* ctx, int on)
 {
     if (!ctx) return IM3D_ERR_INVALID_ARG;
-    ctx->prof = on != 0;
+    ctx->prof = on == 2 ? 2 : (on != 0 ? 1 : 0);
     return IM3D_OK;
 }
 
@@ -2034,6 +2054,7 @@ void im3d_rsfe_params_default(im3d_rsfe_params* p)
     p->conv_cyclic = 0;
     p->reserved_ = 0;
 }
+#endif  // generic entry points
 
 #define IM3D_ENTRY(...)                \
     do {                               \
@@ -2042,26 +2063,12 @@ void im3d_rsfe_params_default(im3d_rsfe_params* p)
         return __VA_ARGS__;            \
     } while (0)
 
-int im3d_gauss_filter_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
-                          double hx, double hy, double hz, double sigma, double radius,
-                          int pixel_approach)
-{
-    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
-}
-
+#if IM3D_UNIT != 2
 int im3d_gauss_filter_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz,
                           double hx, double hy, double hz, double sigma, double radius,
                           int pixel_approach)
 {
     IM3D_ENTRY(gauss_filter<double>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
-}
-
-int im3d_connected_component_f32(im3d_ctx* ctx, const float* img, float* res, int nx, int ny,
-                                 int nz, const float* init, int i, int j, int k, double threshold,
-                                 int full_connected, int binary_output, int* passes)
-{
-    IM3D_ENTRY(connected_component_op<float>(ctx, img, res, nx, ny, nz, init, i, j, k, threshold,
-                                             full_connected, binary_output, passes));
 }
 
 int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, int nx, int ny,
@@ -2072,27 +2079,12 @@ int im3d_connected_component_f64(im3d_ctx* ctx, const double* img, double* res, 
                                               full_connected, binary_output, passes));
 }
 
-int im3d_gauss_filter_cyclic_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny,
-                                 int nz, double hx, double hy, double hz, double sigma,
-                                 double radius, int pixel_approach)
-{
-    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius,
-                                   pixel_approach, 1));
-}
-
 int im3d_gauss_filter_cyclic_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny,
                                  int nz, double hx, double hy, double hz, double sigma,
                                  double radius, int pixel_approach)
 {
     IM3D_ENTRY(gauss_filter<double>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius,
                                     pixel_approach, 1));
-}
-
-int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,
-                            double hx, double hy, double hz, double dt, double bc, int bc_type,
-                            int sweep_order, int sweeps)
-{
-    IM3D_ENTRY(poisson_sweeps<float>(ctx, res, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, sweep_order, sweeps));
 }
 
 int im3d_poisson_sweeps_f64(im3d_ctx* ctx, double* res, const double* b, int nx, int ny, int nz,
@@ -2102,15 +2094,6 @@ int im3d_poisson_sweeps_f64(im3d_ctx* ctx, double* res, const double* b, int nx,
     IM3D_ENTRY(poisson_sweeps<double>(ctx, res, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, sweep_order, sweeps));
 }
 
-int im3d_poisson_solve_f32(im3d_ctx* ctx, float* u, const float* b, int nx, int ny, int nz,
-                           double hx, double hy, double hz, double dt, double bc, int bc_type,
-                           double rel_res_tol, int max_sweeps, int check_every, double omega,
-                           int* sweeps_done, double* rel_res)
-{
-    IM3D_ENTRY(poisson_solve<float>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
-                                    max_sweeps, check_every, omega, sweeps_done, rel_res));
-}
-
 int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, int ny, int nz,
                            double hx, double hy, double hz, double dt, double bc, int bc_type,
                            double rel_res_tol, int max_sweeps, int check_every, double omega,
@@ -2118,6 +2101,75 @@ int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, in
 {
     IM3D_ENTRY(poisson_solve<double>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
                                      max_sweeps, check_every, omega, sweeps_done, rel_res));
+}
+
+int im3d_grad_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
+                  double hy, double hz)
+{
+    IM3D_ENTRY(grad_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_div_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
+                 double hy, double hz)
+{
+    IM3D_ENTRY(div_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
+}
+
+int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, int nx, int ny,
+                        int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
+                        double* phi_out, double* u_out, double* f1_out, double* f2_out,
+                        im3d_rsfe_stats* stats)
+{
+    IM3D_ENTRY(rsfe_apply<double>(ctx, myim, init, nx, ny, nz, hx, hy, hz, p, phi_out, u_out, f1_out,
+                                  f2_out, stats));
+}
+
+int im3d_rsfe_apply_batched_f64(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
+                                const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
+                                double* latency_ms)
+{
+    IM3D_ENTRY(rsfe_apply_batched<double>(ctx, nvol, vols, p, streams, stats, latency_ms));
+}
+#endif  // FP64 entry points
+
+#if IM3D_UNIT != 1
+int im3d_gauss_filter_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz,
+                          double hx, double hy, double hz, double sigma, double radius,
+                          int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius, pixel_approach));
+}
+
+int im3d_connected_component_f32(im3d_ctx* ctx, const float* img, float* res, int nx, int ny,
+                                 int nz, const float* init, int i, int j, int k, double threshold,
+                                 int full_connected, int binary_output, int* passes)
+{
+    IM3D_ENTRY(connected_component_op<float>(ctx, img, res, nx, ny, nz, init, i, j, k, threshold,
+                                             full_connected, binary_output, passes));
+}
+
+int im3d_gauss_filter_cyclic_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny,
+                                 int nz, double hx, double hy, double hz, double sigma,
+                                 double radius, int pixel_approach)
+{
+    IM3D_ENTRY(gauss_filter<float>(ctx, in, out, nx, ny, nz, hx, hy, hz, sigma, radius,
+                                   pixel_approach, 1));
+}
+
+int im3d_poisson_sweeps_f32(im3d_ctx* ctx, float* res, const float* b, int nx, int ny, int nz,
+                            double hx, double hy, double hz, double dt, double bc, int bc_type,
+                            int sweep_order, int sweeps)
+{
+    IM3D_ENTRY(poisson_sweeps<float>(ctx, res, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, sweep_order, sweeps));
+}
+
+int im3d_poisson_solve_f32(im3d_ctx* ctx, float* u, const float* b, int nx, int ny, int nz,
+                           double hx, double hy, double hz, double dt, double bc, int bc_type,
+                           double rel_res_tol, int max_sweeps, int check_every, double omega,
+                           int* sweeps_done, double* rel_res)
+{
+    IM3D_ENTRY(poisson_solve<float>(ctx, u, b, nx, ny, nz, hx, hy, hz, dt, bc, bc_type, rel_res_tol,
+                                    max_sweeps, check_every, omega, sweeps_done, rel_res));
 }
 
 int im3d_gauss_filter_f32_noalloc(const float* in, float* out, int nx, int ny, int nz,
@@ -2134,22 +2186,10 @@ int im3d_grad_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, in
     IM3D_ENTRY(grad_op<float>(ctx, in, out, nx, ny, nz, hx, hy, hz));
 }
 
-int im3d_grad_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
-                  double hy, double hz)
-{
-    IM3D_ENTRY(grad_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
-}
-
 int im3d_div_f32(im3d_ctx* ctx, const float* in, float* out, int nx, int ny, int nz, double hx,
                  double hy, double hz)
 {
     IM3D_ENTRY(div_op<float>(ctx, in, out, nx, ny, nz, hx, hy, hz));
-}
-
-int im3d_div_f64(im3d_ctx* ctx, const double* in, double* out, int nx, int ny, int nz, double hx,
-                 double hy, double hz)
-{
-    IM3D_ENTRY(div_op<double>(ctx, in, out, nx, ny, nz, hx, hy, hz));
 }
 
 int im3d_rsfe_apply_f32(im3d_ctx* ctx, const float* myim, const float* init, int nx, int ny, int nz,
@@ -2160,27 +2200,12 @@ int im3d_rsfe_apply_f32(im3d_ctx* ctx, const float* myim, const float* init, int
                                  f2_out, stats));
 }
 
-int im3d_rsfe_apply_f64(im3d_ctx* ctx, const double* myim, const double* init, int nx, int ny,
-                        int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
-                        double* phi_out, double* u_out, double* f1_out, double* f2_out,
-                        im3d_rsfe_stats* stats)
-{
-    IM3D_ENTRY(rsfe_apply<double>(ctx, myim, init, nx, ny, nz, hx, hy, hz, p, phi_out, u_out, f1_out,
-                                  f2_out, stats));
-}
-
 int im3d_rsfe_apply_batched_f32(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
                                 const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
                                 double* latency_ms)
 {
     IM3D_ENTRY(rsfe_apply_batched<float>(ctx, nvol, vols, p, streams, stats, latency_ms));
 }
-
-int im3d_rsfe_apply_batched_f64(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
-                                const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
-                                double* latency_ms)
-{
-    IM3D_ENTRY(rsfe_apply_batched<double>(ctx, nvol, vols, p, streams, stats, latency_ms));
-}
+#endif  // FP32 entry points
 
 }  // extern "C"

@@ -1917,7 +1917,7 @@ __device__ __forceinline__ long long packed_at(const Dims& d, int i, int j, int 
 
 // The network's inputs, four FP32 volumes x[f][n] (natural layout): the forcing term
 // rhs = b_eff - u_in / dt, the previous solve's u, div(d - b) and phi.
-__global__ void ws_fields_kernel(const float* __restrict__ bpk, const float* __restrict__ upk,
+static __global__ void ws_fields_kernel(const float* __restrict__ bpk, const float* __restrict__ upk,
                                  const float* __restrict__ prevu, const float* __restrict__ divdb,
                                  const float* __restrict__ phi, Dims d, float inv_dt, float* __restrict__ x)
 {
@@ -1934,7 +1934,7 @@ __global__ void ws_fields_kernel(const float* __restrict__ bpk, const float* __r
 
 // u_in += the network's correction y on the cells the solve updates (all cells with
 // Neumann conditions, the interior with Dirichlet ones, whose faces keep their value).
-__global__ void ws_apply_kernel(float* __restrict__ upk, const float* __restrict__ y, Dims d, int dirichlet)
+static __global__ void ws_apply_kernel(float* __restrict__ upk, const float* __restrict__ y, Dims d, int dirichlet)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1945,7 +1945,7 @@ __global__ void ws_apply_kernel(float* __restrict__ upk, const float* __restrict
 }
 
 // The correction the solve made, natural layout: t = u_solved - u_in.
-__global__ void ws_target_kernel(const float* __restrict__ upk, const float* __restrict__ upk0, Dims d,
+static __global__ void ws_target_kernel(const float* __restrict__ upk, const float* __restrict__ upk0, Dims d,
                                  float* __restrict__ t)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;

@@ -19,13 +19,17 @@
  * auto_extract_conn_comp_freq and a cc_init_pixel seed, imp :448-536) runs on the GPU
  * inside the loop.
  *
+ * dumpfrequency writes phi as "<outputname>_<t>" after every dumpfrequency-th iteration
+ * but the last, and "<outputname>_<t>_final" at the end (imp :1940-1951, :1967-1979):
+ * the loop hands phi to the host on those iterations only (im3d_ctx_set_observer).
+ *
  * Not on this backend: interactive display (showfrequency, on-the-go updates) and the
- * interactive choice of a connected component, per-iteration dumps (dumpfrequency
- * writes only the final level set, "<outputname>_<t>_final"), 2-D images.
+ * interactive choice of a connected component, 2-D images.
  */
 #ifndef IM3D_RSFE_SPLITBREGMAN_HXX
 #define IM3D_RSFE_SPLITBREGMAN_HXX
 
+#include <algorithm>
 #include <cstdio>
 #include <sstream>
 #include <string>
@@ -342,6 +346,19 @@ public:
     void apply (im3d::image3d<T> const& myim, im3d::image3d<T> const& init) { run (myim, &init); }
 
 private:
+    // the dump of imp :1940-1951, called by the GPU loop with a host copy of phi
+    static int dump_observer (void* user, im3d_rsfe_checkpoint const* ck)
+    {
+        rsfe_splitbregman* self = static_cast<rsfe_splitbregman*> (user);
+        T const* src = static_cast<T const*> (ck->phi);
+        std::copy (src, src + (size_t) self->dimx * self->dimy * self->dimz, self->phi.data() );
+        self->levelset.convertfromimage3d (self->phi);
+        std::ostringstream oss;
+        oss << self->outputname << "_" << ck->t;
+        self->levelset.write (oss.str() );
+        return 0;
+    }
+
     void run (im3d::image3d<T> const& myim, im3d::image3d<T> const* init)
     {
         FILE* redirected = nullptr;
@@ -415,9 +432,13 @@ private:
 
         this->phi.setdim (dimx, dimy, dimz);
         this->phi.seth (myim.gethx(), myim.gethy(), myim.gethz() );
-        const int st = im3d::b200::ops<T>::apply (im3d::b200::context(), myim.data(), ini, dimx, dimy,
+        im3d_ctx* bctx = im3d::b200::context();
+        if (bctx && dumpfrequency > 0)
+            im3d_ctx_set_observer (bctx, (int) dumpfrequency, 0, &rsfe_splitbregman::dump_observer, this);
+        const int st = im3d::b200::ops<T>::apply (bctx, myim.data(), ini, dimx, dimy,
                                                   dimz, myim.gethx(), myim.gethy(), myim.gethz(), &p,
                                                   this->phi.data(), &last_stats);
+        if (bctx && dumpfrequency > 0) im3d_ctx_set_observer (bctx, 0, 0, nullptr, nullptr);
         if (!im3d::b200::failed (st, "apply") )
         {
             if (verbosity)

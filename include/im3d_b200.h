@@ -152,7 +152,9 @@ int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value);
  * bracketed by CUDA events on the launching stream. im3d_ctx_profile() synchronises,
  * writes up to max_entries stage names ('\n'-separated into names), total ms and
  * launch counts, returns the number of stages (negative status on error) and clears
- * the totals when reset != 0. No counterpart in the reference (it has no timers). */
+ * the totals when reset != 0. on == 2 times only each Poisson solve as a whole (stage
+ * "poisson_solve", warm start included), with no events between the launches inside it,
+ * so that they keep their overlap. No counterpart in the reference (it has no timers). */
 int im3d_ctx_set_profiling(im3d_ctx* ctx, int on);
 int im3d_ctx_profile(im3d_ctx* ctx, char* names, int names_cap, double* ms, int64_t* counts,
                      int max_entries, int reset);

@@ -111,6 +111,12 @@ def test_cli_segments_a_metaimage(tmp_path, pkg, O):
     # the driver rescales the image to [0, 255] (examples/rsfe_splitbregman.cxx:86)
     x = u0.astype(np.float32).astype(np.float64)
     x = (x - x.min()) / ((x - x.min()).max() / 255.0)
-    want = O.rsfe_apply(x, None, O.default_params(maxiter=6, sigma=2.0, lamda=0.5, lamda1=1.0,
-                                                  lamda2=1.0, bc=O.BC_DIR, ls_steps=1, tol=0.0))
+    kw = dict(sigma=2.0, lamda=0.5, lamda1=1.0, lamda2=1.0, bc=O.BC_DIR, ls_steps=1, tol=0.0)
+    want = O.rsfe_apply(x, None, O.default_params(maxiter=6, **kw))
     assert rel(phi, want["phi"]) < 1e-9
+    # the per-iteration dumps of the reference's loop: every iteration but the last
+    names = sorted(f for f in os.listdir(tmp_path) if f.startswith("res_") and f.endswith(".mhd"))
+    assert names == ["res_1.mhd", "res_2.mhd", "res_3.mhd", "res_4.mhd", "res_5.mhd", "res_6_final.mhd"]
+    phi3, _ = mhd.read(str(tmp_path / "res_3.mhd"))
+    want3 = O.rsfe_apply(x, None, O.default_params(maxiter=3, **kw))
+    assert rel(phi3, want3["phi"]) < 1e-9
