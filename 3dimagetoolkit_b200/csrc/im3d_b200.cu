@@ -1216,6 +1216,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             st.d = d;
             st.l12 = (T)(p->lamda1 - p->lamda2);
             st.lamda = (T)p->lamda;
+            st.inv_lamda = (T)(1.0 / p->lamda);
             st.inv_dt = (T)(1.0 / p->dt);
             st.bc = (T)chosen_bc;
             st.mode = lex ? 0 : (solve ? 2 : 1);

@@ -212,6 +212,7 @@ struct StRhs {
     double* beff2;
     Dims d;
     T l12, lamda, inv_dt, bc;
+    T inv_lamda;  // FP32 multiplies by it instead of dividing (same value when lamda is a power of two)
     int mode, dirichlet;
     struct Pre {
         T u[4], kn[4], dv[4], ph[4];
@@ -241,7 +242,8 @@ struct StRhs {
             f -= a;
         }
         f -= v.v[1];
-        f /= lamda;
+        if constexpr (sizeof(T) == 4) f *= inv_lamda;
+        else f /= lamda;
         f -= w.dv[r];
         return f;
     }
@@ -307,7 +309,8 @@ struct StRhs {
             r -= a;
         }
         r -= v.v[1];
-        r /= lamda;
+        if constexpr (sizeof(T) == 4) r *= inv_lamda;
+        else r /= lamda;
         r -= ld_g(divdb + q);
         if (mode == 0) {
             out[q] = r;
@@ -446,12 +449,34 @@ __device__ __forceinline__ void window_conv(const T (&x)[R + 2 * S], const T (&w
     }
 }
 
+// The same on two fields at once with the packed f32x2 instructions of sm_100 (the
+// operations of window_conv, lane by lane: identical results, half the instructions).
+template <int S, int R>
+__device__ __forceinline__ void window_conv2(const float2 (&x)[R + 2 * S], const float2 (&w)[S + 1],
+                                             float2 (&out)[R])
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        float2 acc = __fmul2_rn(w[S], x[r + S]);
+#pragma unroll
+        for (int t = 0; t < S; ++t) acc = __ffma2_rn(w[t], __fadd2_rn(x[r + t], x[r + 2 * S - t]), acc);
+        out[r] = acc;
+    }
+}
+
 template <typename T, int S>
 __device__ __forceinline__ void load_taps(const T* __restrict__ taps, T (&w)[S + 1])
 {
 #pragma unroll
     for (int t = 0; t <= S; ++t) w[t] = __ldg(taps + t);
 }
+
+// FP32 passes with an even number of fields keep them in shared memory as float pairs
+// and convolve a pair per packed instruction
+template <typename T, int N>
+struct PairedFields {
+    static constexpr bool value = sizeof(T) == 4 && N % 2 == 0;
+};
 
 // Along k (contiguous). Block TKT x RKR threads; each thread 4 consecutive k of one
 // row; tile RKR rows x 4*TKT k. The halo is rounded up to SP = 4*ceil(S/4) so that
@@ -495,8 +520,15 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.x + u * TKT;
             if (s < W) {
+                if constexpr (PairedFields<T, N>::value) {
+                    float2* sm2 = reinterpret_cast<float2*>(sm);  // [N/2][RKR][W] pairs
 #pragma unroll
-                for (int q = 0; q < N; ++q) sm[(q * RKR + threadIdx.y) * W + s] = v[u].v[q];
+                    for (int q = 0; q < N / 2; ++q)
+                        sm2[(q * RKR + threadIdx.y) * W + s] = make_float2(v[u].v[2 * q], v[u].v[2 * q + 1]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < N; ++q) sm[(q * RKR + threadIdx.y) * W + s] = v[u].v[q];
+                }
             }
         }
     }
@@ -505,7 +537,34 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     __syncthreads();
     const bool act = live && kk < d.nz;
     T res[N][R];
-    if (act) {
+    if constexpr (PairedFields<T, N>::value) {
+        if (act) {
+            float2 w2[S + 1];
+#pragma unroll
+            for (int t = 0; t <= S; ++t) w2[t] = make_float2(w[t], w[t]);
+#pragma unroll
+            for (int q = 0; q < N / 2; ++q) {
+                const float2* base = reinterpret_cast<const float2*>(sm) + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
+                float2 xa[XW];
+#pragma unroll
+                for (int t = 0; t < XW; t += 2) {
+                    const float4 v4 = *reinterpret_cast<const float4*>(base + t);
+                    xa[t] = make_float2(v4.x, v4.y);
+                    xa[t + 1] = make_float2(v4.z, v4.w);
+                }
+                float2 x[R + 2 * S];
+#pragma unroll
+                for (int t = 0; t < R + 2 * S; ++t) x[t] = xa[t + SP - S];
+                float2 o[R];
+                window_conv2<S, R>(x, w2, o);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    res[2 * q][r] = o[r].x;
+                    res[2 * q + 1][r] = o[r].y;
+                }
+            }
+        }
+    } else if (act) {
 #pragma unroll
         for (int q = 0; q < N; ++q) {
             const T* base = sm + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
@@ -568,8 +627,15 @@ __global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.y + u * TY;
             if (s < H) {
+                if constexpr (PairedFields<T, N>::value) {
+                    float2* sm2 = reinterpret_cast<float2*>(sm);  // [N/2][H][TW] pairs
 #pragma unroll
-                for (int q = 0; q < N; ++q) sm[(q * H + s) * TW + threadIdx.x] = v[u].v[q];
+                    for (int q = 0; q < N / 2; ++q)
+                        sm2[(q * H + s) * TW + threadIdx.x] = make_float2(v[u].v[2 * q], v[u].v[2 * q + 1]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < N; ++q) sm[(q * H + s) * TW + threadIdx.x] = v[u].v[q];
+                }
             }
         }
     }
@@ -579,6 +645,25 @@ __global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d
     if (!kin) return;
     const int r0 = threadIdx.y * R;
     Vec<T, N> out[R];
+    if constexpr (PairedFields<T, N>::value) {
+        float2 w2[S + 1];
+#pragma unroll
+        for (int t = 0; t <= S; ++t) w2[t] = make_float2(w[t], w[t]);
+        const float2* sm2 = reinterpret_cast<const float2*>(sm);
+#pragma unroll
+        for (int q = 0; q < N / 2; ++q) {
+            float2 x[R + 2 * S];
+#pragma unroll
+            for (int t = 0; t < R + 2 * S; ++t) x[t] = sm2[(q * H + r0 + t) * TW + threadIdx.x];
+            float2 o[R];
+            window_conv2<S, R>(x, w2, o);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                out[r].v[2 * q] = o[r].x;
+                out[r].v[2 * q + 1] = o[r].y;
+            }
+        }
+    } else {
 #pragma unroll
     for (int q = 0; q < N; ++q) {
         T x[R + 2 * S];
@@ -588,6 +673,7 @@ __global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d
         window_conv<T, S, R>(x, w, o);
 #pragma unroll
         for (int r = 0; r < R; ++r) out[r].v[q] = o[r];
+    }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -898,6 +984,17 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_kernel(const Vec<T, 4>* __r
 }
 
 // ------------------------------------------------------------------ stencils
+// x / (2h) of the difference stencils: FP64 divides, with the reference's operations;
+// FP32 multiplies by the reciprocal, which gives the same value when 2h is a power of
+// two (unit spacing) and is within 1 ulp of it otherwise, at a fraction of a
+// division's instructions.
+template <typename T>
+__device__ __forceinline__ T over_two_h(T x, T two_h, T inv_two_h)
+{
+    if constexpr (sizeof(T) == 4) return x * inv_two_h;
+    else return x / two_h;
+}
+
 // One component of image3d::grad at a point with position pos on an axis of length
 // len (image3d_imp.hxx:762-838): central inside, one-sided second order on faces.
 template <typename T>
@@ -1521,6 +1618,7 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
     const long long sy = d.nz;
     const long long n = d.n();
     const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    const T ihx = T(1. / (2. * hx)), ihy = T(1. / (2. * hy)), ihz = T(1. / (2. * hz));
     const bool jint = j >= 1 && j <= d.ny - 2;
     const long long p0 = d.idx(i0, j, kb);
     VV f[NI + 2];
@@ -1530,27 +1628,46 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
         if (i >= 0 && i < d.nx) f[t] = *reinterpret_cast<const VV*>(phi + p0 + (long long)(t - 1) * plane);
         else f[t] = VV{};
     }
+    // every read of the NI planes is issued before the first store: b3 is read and
+    // written, so a read placed after a store could not be moved ahead of it
+    VV yms[NI], yps[NI], ggs[NI], bos[NI][3];
+    T zlo[NI], zhi[NI];
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        const int i = i0 + t;
+        const long long p = p0 + (long long)t * plane;
+        yms[t] = yps[t] = ggs[t] = VV{};
+        bos[t][0] = bos[t][1] = bos[t][2] = VV{};
+        zlo[t] = zhi[t] = T(0);
+        if (i < d.nx) {
+            if (jint && i >= 1 && i <= d.nx - 2) {
+                yms[t] = *reinterpret_cast<const VV*>(phi + p - sy);
+                yps[t] = *reinterpret_cast<const VV*>(phi + p + sy);
+            }
+            if (kb >= 1) zlo[t] = phi[p - 1];
+            if (kb + W < d.nz) zhi[t] = phi[p + W];
+            ggs[t] = *reinterpret_cast<const VV*>(g3 + p);
+#pragma unroll
+            for (int cmp = 0; cmp < 3; ++cmp) bos[t][cmp] = *reinterpret_cast<const VV*>(b3 + cmp * n + p);
+        }
+    }
 #pragma unroll
     for (int t = 0; t < NI; ++t) {
         const int i = i0 + t;
         if (i >= d.nx) break;
         const long long p = p0 + (long long)t * plane;
         const bool rowint = jint && i >= 1 && i <= d.nx - 2;
-        VV ym = VV{}, yp = VV{};
-        if (rowint) {
-            ym = *reinterpret_cast<const VV*>(phi + p - sy);
-            yp = *reinterpret_cast<const VV*>(phi + p + sy);
-        }
+        const VV ym = yms[t], yp = yps[t];
         // phi at k = kb-1 .. kb+W of this row: zz[c + 1] = phi[kb + c]
         T zz[W + 2];
-        zz[0] = kb >= 1 ? phi[p - 1] : T(0);
+        zz[0] = zlo[t];
 #pragma unroll
         for (int c = 0; c < W; ++c) zz[c + 1] = VT::get(f[t + 1], c);
-        zz[W + 1] = kb + W < d.nz ? phi[p + W] : T(0);
-        const VV gg = *reinterpret_cast<const VV*>(g3 + p);
+        zz[W + 1] = zhi[t];
+        const VV gg = ggs[t];
         VV bo[3], dn[3];
 #pragma unroll
-        for (int cmp = 0; cmp < 3; ++cmp) bo[cmp] = *reinterpret_cast<const VV*>(b3 + cmp * n + p);
+        for (int cmp = 0; cmp < 3; ++cmp) bo[cmp] = bos[t][cmp];
 #pragma unroll
         for (int cc = 0; cc < W; ++cc) {
             const int k = kb + cc;
@@ -1559,15 +1676,15 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
                 // i and j inside: central x and y terms; the z term is central or, on
                 // the faces k = 0 and k = nz-1, grad_term's one-sided difference,
                 // evaluated with the same operations without a branch
-                gr[0] = (VT::get(f[t + 2], cc) - VT::get(f[t], cc)) / two_hx;
-                gr[1] = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
-                T tz = (zz[cc + 2] - zz[cc]) / two_hz;
+                gr[0] = over_two_h(VT::get(f[t + 2], cc) - VT::get(f[t], cc), two_hx, ihx);
+                gr[1] = over_two_h(VT::get(yp, cc) - VT::get(ym, cc), two_hy, ihy);
+                T tz = over_two_h(zz[cc + 2] - zz[cc], two_hz, ihz);
                 if (cc == 0) {
-                    const T lo = (T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3]) / two_hz;
+                    const T lo = over_two_h(T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3], two_hz, ihz);
                     tz = k == 0 ? lo : tz;
                 }
                 if (cc == W - 1) {
-                    const T hi = (T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1]) / two_hz;
+                    const T hi = over_two_h(T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1], two_hz, ihz);
                     tz = k == d.nz - 1 ? hi : tz;
                 }
                 gr[2] = tz;
@@ -1619,6 +1736,7 @@ __global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T
     const T* f1 = v + n;
     const T* f2 = v + 2 * n;
     const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    const T ihx = T(1. / (2. * hx)), ihy = T(1. / (2. * hy)), ihz = T(1. / (2. * hz));
     const bool jint = j >= 1 && j <= d.ny - 2;
     const long long p0 = d.idx(i0, j, kb);
     VV x[NI + 2];
@@ -1651,15 +1769,15 @@ __global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T
 #pragma unroll
             for (int cc = 0; cc < W; ++cc) {
                 const int k = kb + cc;
-                const T tx = (VT::get(x[t + 2], cc) - VT::get(x[t], cc)) / two_hx;
-                const T ty = (VT::get(yp, cc) - VT::get(ym, cc)) / two_hy;
-                T tz = (zz[cc + 2] - zz[cc]) / two_hz;
+                const T tx = over_two_h(VT::get(x[t + 2], cc) - VT::get(x[t], cc), two_hx, ihx);
+                const T ty = over_two_h(VT::get(yp, cc) - VT::get(ym, cc), two_hy, ihy);
+                T tz = over_two_h(zz[cc + 2] - zz[cc], two_hz, ihz);
                 if (cc == 0) {
-                    const T lo = (T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3]) / two_hz;
+                    const T lo = over_two_h(T(4) * zz[cc + 2] - T(3) * zz[cc + 1] - zz[cc + 3], two_hz, ihz);
                     tz = k == 0 ? lo : tz;
                 }
                 if (cc == W - 1) {
-                    const T hi = (T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1]) / two_hz;
+                    const T hi = over_two_h(T(3) * zz[cc + 1] - T(4) * zz[cc] + zz[cc - 1], two_hz, ihz);
                     tz = k == d.nz - 1 ? hi : tz;
                 }
                 VT::set(o, cc, tx + ty + tz);

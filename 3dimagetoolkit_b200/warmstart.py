@@ -141,7 +141,7 @@ def main(argv=None):
     import json
 
     ap = argparse.ArgumentParser(description="train or evaluate the learned Poisson warm start")
-    ap.add_argument("what", choices=["train", "evaluate"])
+    ap.add_argument("what", choices=["train", "evaluate", "forward"])
     ap.add_argument("--seeds", default="0-199", help="first-last (inclusive)")
     ap.add_argument("--size", type=int, default=0, help="cube side (train 128, evaluate 256)")
     ap.add_argument("--maxiter", type=int, default=100)
@@ -168,6 +168,23 @@ def main(argv=None):
                  pairs=res["pairs"], losses=np.array(res["losses"]), seconds=res["seconds"])
             print(json.dumps({"pairs": res["pairs"], "seconds": res["seconds"],
                               "first_loss": res["losses"][0], "last_loss": res["losses"][-1]}))
+        elif a.what == "forward":
+            # device time of one inference on random fields (CUDA events, median of 5)
+            import torch
+
+            side = a.size or 256
+            x = torch.randn((1, 4, side, side, side), device="cuda", dtype=torch.float32)
+            ts = []
+            for q in range(7):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                net.forward(x)
+                e1.record()
+                e1.synchronize()
+                if q >= 2:
+                    ts.append(e0.elapsed_time(e1))
+            print(json.dumps({"size": side, "forward_ms": sorted(ts)[len(ts) // 2]}))
         else:
             load(net, a.weights)
             side = a.size or 256

@@ -256,3 +256,10 @@ def ref_last_timeline():
     buf = np.zeros(100000)
     n = ref_lib().ref_last_timeline(_p(buf), C.c_int(buf.size))
     return buf[:n].copy()
+
+
+def ref_last_sweep_marks():
+    """Sweeps run up to the end of each outer iteration's Poisson step (last run)."""
+    buf = np.zeros(100000)
+    n = ref_lib().ref_last_sweep_marks(_p(buf), C.c_int(buf.size))
+    return buf[:n].copy()

@@ -66,10 +66,11 @@ struct Recorder
     double last_rel = -1;
     int not_converged = 0;
     std::vector<double> stamps;  // wall clock (s) at the end of each Poisson step
+    std::vector<double> marks;   // sweeps run up to the end of each Poisson step
 };
 
 Recorder g_rec;
-std::vector<double> g_last_stamps;
+std::vector<double> g_last_stamps, g_last_marks;
 double g_apply_start = 0, g_apply_end = 0;
 
 double now_s()
@@ -162,6 +163,7 @@ void rec_poisson (img& res, img const& b, double const& dt, double const& bc, im
     }
     g_rec.u = res;
     g_rec.stamps.push_back(now_s() );
+    g_rec.marks.push_back( (double) g_rec.sweeps);
 }
 
 }  // namespace
@@ -378,6 +380,7 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     else algo.apply (u0);
     g_apply_end = now_s();
     g_last_stamps = g_rec.stamps;
+    g_last_marks = g_rec.marks;
 
     img phi = algo.getoutput();
     if (phi_out) from_img (phi_out, phi);
@@ -419,6 +422,16 @@ int ref_last_timeline (double* out, int cap)
     for (double t : g_last_stamps)
         if (n < cap) out[n++] = t;
     if (n < cap) out[n++] = g_apply_end;
+    return n;
+}
+
+/* Sweeps of the last ref_rsfe_apply: out[n] = sweeps run up to the end of the n-th
+ * outer iteration's Poisson step. Returns the number of values written. */
+int ref_last_sweep_marks (double* out, int cap)
+{
+    int n = 0;
+    for (double m : g_last_marks)
+        if (n < cap) out[n++] = m;
     return n;
 }
 

@@ -39,7 +39,7 @@ def layout():
 
 
 def bf16(t):
-    return t.to(torch.bfloat16).to(torch.float32)
+    return t.to(torch.bfloat16).to(t.dtype)
 
 
 def round_st(t):
@@ -89,7 +89,7 @@ def forward(x, ps, emulate_bf16=True, hooks=False):
         z = gh(F.conv3d(t, rd(w), ps[name + ".b"], padding=1))  # its gradient: stored in BF16
         return rd(F.relu(z))
 
-    x0 = rd(torch.cat([x, torch.zeros((x.shape[0], 12) + tuple(x.shape[2:]))], 1))
+    x0 = rd(torch.cat([x, torch.zeros((x.shape[0], 12) + tuple(x.shape[2:]), dtype=x.dtype)], 1))
     a1 = conv(x0, "e1a")
     a = conv(a1, "e1b")
     p1 = gh(F.max_pool3d(a, 2))
