@@ -597,22 +597,104 @@ def run_batch(args):
 
 
 # ------------------------------------------------------------------ CPU arms
-def _ref_iteration_seconds(shape, maxiter, seed):
-    """Wall seconds of each outer iteration after the first, reference code, FP64."""
-    import numpy as np
+REF_FIXTURE = os.path.join(ROOT, "tests", "golden", "rsfe_c2_256_ref.npz")
 
+
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
 
+    return O
+
+
+def _ref_iterations(shape, maxiter, seed, threads):
+    """Runs the reference's own code (FP64) on the 256^3 workload for maxiter outer
+    iterations with `threads` OpenMP threads; returns, per outer iteration after the
+    first, its wall seconds, the seconds inside its Poisson step and inside FFTs, and
+    its sweeps."""
+    import numpy as np
+
+    O = _oracle()
+    O.set_threads(threads)
     pkg = importlib.import_module("3dimagetoolkit_b200")
     u0, phi0 = pkg.synth.config_volume("c2", seed=seed, dtype=np.float64)
     kw = dict(PARAMS)
     kw["maxiter"] = maxiter
-    p = O.default_params(**kw)
-    O.rsfe_apply(u0, phi0, p, use_reference=True)
-    tl = O.ref_last_timeline()
-    steps = np.diff(tl[1:-1])  # end-of-iteration stamps: intervals are whole iterations
-    return [float(x) for x in steps]
+    O.rsfe_apply(u0, phi0, O.default_params(**kw), use_reference=True)
+    ends = O.ref_last_timeline()[1:-1]  # end of each outer iteration's Poisson step
+    marks = O.ref_last_sweep_marks()
+    solve, fft = O.ref_last_step_profile()
+    # iteration q runs from the end of step q-1 to the end of step q: the rest of
+    # iteration q-1 (clamp, tolerance, Bregman, div) and the start and solve of q
+    return [{"seconds": float(ends[q] - ends[q - 1]), "solve": float(solve[q]),
+             "fft": float(fft[q] - fft[q - 1]), "sweeps": float(marks[q] - marks[q - 1])}
+            for q in range(1, len(ends))]
+
+
+def _fftw_probe() -> str:
+    import ctypes.util
+
+    libs = [n for n in ("fftw3", "fftw3_omp", "fftw3_threads") if ctypes.util.find_library(n)]
+    return ("found: " + ", ".join(libs)) if libs else "absent (no libfftw3 on this host)"
+
+
+def _fft_seconds(threads):
+    """One 274^3 complex FP64 transform (the size the reference's 256^3 convolutions
+    pad to): the in-tree FFT behind the reference's FFTW calls, and scipy's pocketfft
+    (ducc) with the same threads, for scale."""
+    import numpy as np
+
+    O = _oracle()
+    O.set_threads(threads)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((274, 274, 274)) + 1j * rng.standard_normal((274, 274, 274))
+    O.ref_fft3d(x)
+    t0 = time.perf_counter()
+    O.ref_fft3d(x)
+    shim = time.perf_counter() - t0
+    try:
+        import scipy.fft
+
+        scipy.fft.fftn(x, workers=threads)
+        t0 = time.perf_counter()
+        scipy.fft.fftn(x, workers=threads)
+        ducc = time.perf_counter() - t0
+    except ImportError:
+        ducc = None
+    return shim, ducc
+
+
+def _ref_summary(its, threads, n):
+    """The reference arm's figures from measured outer iterations."""
+    import numpy as np
+
+    tot = sum(r["seconds"] for r in its)
+    solve = sum(r["solve"] for r in its)
+    fft = sum(r["fft"] for r in its)
+    sweeps = sum(r["sweeps"] for r in its)
+    k = len(its)
+    per_sweep = solve / max(sweeps, 1)
+    out = {
+        "value": n * k / tot / 1e9,
+        "seconds_per_iteration": tot / k,
+        "breakdown_s_per_iteration": {"fft": fft / k, "poisson_solve": solve / k,
+                                      "other": (tot - fft - solve) / k},
+        "sweeps_per_iteration": sweeps / k,
+        "seconds_per_sweep": per_sweep,
+        "threads": threads,
+        "fftw": _fftw_probe(),
+    }
+    # The timed iterations are early ones; the full 100-iteration run (the GPU arm's
+    # step) has its own sweep profile, recorded by the reference in the 256^3 fixture.
+    if os.path.exists(REF_FIXTURE):
+        d = np.load(REF_FIXTURE)
+        s_full = float(d["total_sweeps"]) / float(d["iterations"])
+        per_it = (tot - solve) / k + per_sweep * s_full
+        out["same_profile"] = {
+            "sweeps_per_iteration": s_full,
+            "source": "the reference's own 100-iteration 256^3 run (tests/golden/rsfe_c2_256_ref.npz)",
+            "seconds_per_iteration": per_it, "value": n / per_it / 1e9}
+    return out
 
 
 def _cpu_model() -> str:
@@ -626,41 +708,49 @@ def _cpu_model() -> str:
 
 
 def cpu_baseline(args):
-    cores = os.cpu_count()
+    threads = args.ref_threads or os.cpu_count()
     t0 = time.time()
-    secs = _ref_iteration_seconds(SHAPE, 2, args.seed)
+    its = _ref_iterations(SHAPE, 2, args.seed, threads)
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
-    per_it = statistics.median(secs)
-    log(f"cpu baseline: {len(secs)} timed iteration(s), {per_it:.2f} s each, "
+    summ = _ref_summary(its, threads, n)
+    log(f"cpu baseline: {len(its)} timed iteration(s), {summ['seconds_per_iteration']:.2f} s each, "
         f"{time.time() - t0:.1f} s total")
-    return {"value": n / per_it / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
-            "cpu_model": _cpu_model(),
+    return {"value": summ["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "cpu_model": _cpu_model(), **{k: v for k, v in summ.items() if k != "value"},
             "sample": "reference C++ (oracle/_ref: the reference headers, FFTW replaced by an "
                       "in-tree FP64 FFT, VTK/GetPot by headless shims), T=double, 256^3, "
-                      "wall time of outer iteration 2 of 2 (setup and iteration 1 excluded), "
-                      f"OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)}"}
+                      "wall time of outer iteration 2 of 2 (setup and iteration 1 excluded)"}
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    cores = os.cpu_count()
+    threads = args.ref_threads or os.cpu_count()
     maxiter = 1 + args.warmup + args.steps
-    secs = _ref_iteration_seconds(SHAPE, maxiter, args.seed)
-    timed = secs[args.warmup:args.warmup + args.steps] if len(secs) > args.warmup else secs
-    total = sum(timed)
+    its = _ref_iterations(SHAPE, maxiter, args.seed, threads)
+    timed = its[args.warmup:args.warmup + args.steps] if len(its) > args.warmup else its
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
-    value = n * len(timed) / total / 1e9
+    summ = _ref_summary(timed, threads, n)
+    shim, ducc = _fft_seconds(threads)
+    fft_it = summ["breakdown_s_per_iteration"]["fft"]
+    summ["fft_274cube_seconds"] = {"in_tree": shim, "scipy_pocketfft": ducc}
+    if ducc and "same_profile" in summ:
+        # the same iterations with every FFT at pocketfft's speed: what an FFTW-class
+        # library would give the reference, a bound on the in-tree FFT's share
+        per_it = summ["same_profile"]["seconds_per_iteration"] - fft_it * (1 - ducc / shim)
+        summ["same_profile"]["value_with_pocketfft_speed"] = n / per_it / 1e9
+    value = summ.pop("value")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
-        "steps": len(timed), "warmup": args.warmup, "ms_per_step": total / len(timed) * 1e3,
+        "steps": len(timed), "warmup": args.warmup,
+        "ms_per_step": summ["seconds_per_iteration"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded ellipsoid volume)",
         "config": {"workload": "rsfe-sb 256^3, one outer iteration per step, Poisson step solved "
                                "to rel. residual 1e-6 (red-black plug-in)", "shape": list(SHAPE)},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "cpu_model": _cpu_model(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "cpu_model": _cpu_model(), "host_cores": os.cpu_count(), **summ,
                          "sample": f"{len(timed)} outer iterations of the 256^3 workload after "
                                    f"{args.warmup} warm-up iterations and the set-up"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -676,6 +766,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ref-threads", type=int, default=0,
+                    help="OpenMP threads of the reference's CPU code (default: all host cores)")
     ap.add_argument("--no-unet", action="store_true",
                     help="skip timing the library network behind the warm-start bound")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batch"],

@@ -263,3 +263,27 @@ def ref_last_sweep_marks():
     buf = np.zeros(100000)
     n = ref_lib().ref_last_sweep_marks(_p(buf), C.c_int(buf.size))
     return buf[:n].copy()
+
+
+def ref_last_step_profile():
+    """(solve, fft) per outer iteration of the last run: wall seconds inside its Poisson
+    step, and FFT wall seconds accumulated up to the end of that step."""
+    solve = np.zeros(100000)
+    fft = np.zeros(100000)
+    n = ref_lib().ref_last_step_profile(_p(solve), _p(fft), C.c_int(solve.size))
+    return solve[:n].copy(), fft[:n].copy()
+
+
+def ref_fft_totals():
+    """(seconds, calls) spent in the FFT shim's fftw_execute since the library loaded."""
+    s = C.c_double(0)
+    n = C.c_longlong(0)
+    ref_lib().im3d_fft_shim_totals(C.byref(s), C.byref(n))
+    return s.value, n.value
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of the checker's and the reference's parallel regions started from
+    the calling thread (omp_set_num_threads of the libgomp both libraries use)."""
+    ref_lib()
+    C.CDLL("libgomp.so.1").omp_set_num_threads(C.c_int(int(n)))

@@ -179,6 +179,10 @@ struct im3d_fft_plan_s {
 };
 
 static int g_nthreads = 0;
+static double g_exec_seconds = 0;  // wall time spent in fftw_execute since the library loaded
+static long long g_exec_calls = 0;
+
+static void execute_3d(im3d_fft_plan_s* p);
 
 extern "C" {
 
@@ -200,7 +204,24 @@ fftw_plan fftw_plan_dft_3d(int n0, int n1, int n2, fftw_complex* in, fftw_comple
 
 void fftw_execute(const fftw_plan pc)
 {
-    im3d_fft_plan_s* p = pc;
+    const double t0 = omp_get_wtime();
+    execute_3d(pc);
+    g_exec_seconds += omp_get_wtime() - t0;
+    ++g_exec_calls;
+}
+
+/* Wall seconds spent in fftw_execute and the number of its calls since the library
+ * loaded (the CPU baseline's FFT share of an outer iteration). */
+void im3d_fft_shim_totals(double* seconds, long long* calls)
+{
+    if (seconds) *seconds = g_exec_seconds;
+    if (calls) *calls = g_exec_calls;
+}
+
+}  // extern "C"
+
+static void execute_3d(im3d_fft_plan_s* p)
+{
     const long n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
     const long total = n0 * n1 * n2;
     if (p->out != p->in) std::memcpy(p->out, p->in, sizeof(cplx) * total);
@@ -249,6 +270,8 @@ void fftw_execute(const fftw_plan pc)
         }
     }
 }
+
+extern "C" {
 
 void fftw_destroy_plan(fftw_plan p)
 {

@@ -24,6 +24,9 @@
 #include <cstring>
 #include <vector>
 
+// fft_shim.cpp: wall seconds spent in fftw_execute and its call count
+extern "C" void im3d_fft_shim_totals(double* seconds, long long* calls);
+
 namespace {
 
 typedef im3d::image3d<double> img;
@@ -67,10 +70,12 @@ struct Recorder
     int not_converged = 0;
     std::vector<double> stamps;  // wall clock (s) at the end of each Poisson step
     std::vector<double> marks;   // sweeps run up to the end of each Poisson step
+    std::vector<double> solve_s; // wall seconds inside each Poisson step
+    std::vector<double> fft_s;   // FFT wall seconds (fft_shim.cpp) up to the end of each step
 };
 
 Recorder g_rec;
-std::vector<double> g_last_stamps, g_last_marks;
+std::vector<double> g_last_stamps, g_last_marks, g_last_solve, g_last_fft;
 double g_apply_start = 0, g_apply_end = 0;
 
 double now_s()
@@ -117,6 +122,7 @@ void record_conv (img const& result)
 
 void rec_poisson (img& res, img const& b, double const& dt, double const& bc, img const& input)
 {
+    const double t_enter = now_s();
     const int nx = res.getdimx(), ny = res.getdimy(), nz = res.getdimz();
     if (g_rec.mode == 0)
     {
@@ -164,6 +170,10 @@ void rec_poisson (img& res, img const& b, double const& dt, double const& bc, im
     g_rec.u = res;
     g_rec.stamps.push_back(now_s() );
     g_rec.marks.push_back( (double) g_rec.sweeps);
+    g_rec.solve_s.push_back(g_rec.stamps.back() - t_enter);
+    double fft_seconds = 0;
+    im3d_fft_shim_totals(&fft_seconds, nullptr);
+    g_rec.fft_s.push_back(fft_seconds);
 }
 
 }  // namespace
@@ -381,6 +391,8 @@ int ref_rsfe_apply (const double* myim, const double* init, int nx, int ny, int 
     g_apply_end = now_s();
     g_last_stamps = g_rec.stamps;
     g_last_marks = g_rec.marks;
+    g_last_solve = g_rec.solve_s;
+    g_last_fft = g_rec.fft_s;
 
     img phi = algo.getoutput();
     if (phi_out) from_img (phi_out, phi);
@@ -432,6 +444,20 @@ int ref_last_sweep_marks (double* out, int cap)
     int n = 0;
     for (double m : g_last_marks)
         if (n < cap) out[n++] = m;
+    return n;
+}
+
+/* Per outer iteration of the last ref_rsfe_apply: solve[n] = wall seconds inside its
+ * Poisson step, fft[n] = wall seconds spent in FFTs (since the library loaded) up to
+ * the end of that step. Returns the number of iterations written. */
+int ref_last_step_profile (double* solve, double* fft, int cap)
+{
+    int n = 0;
+    for (; n < (int) g_last_solve.size() && n < cap; ++n)
+    {
+        solve[n] = g_last_solve[n];
+        fft[n] = g_last_fft[n];
+    }
     return n;
 }
 

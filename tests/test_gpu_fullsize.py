@@ -78,8 +78,10 @@ def _fixture_case(pkg):
 def test_fp64_matches_the_reference_at_256(ctx, pkg):
     """The FP64 path against the reference's own run of the 256^3 workload (100 outer
     iterations, each solve to relative residual 1e-6): the same iteration, sweep and
-    residual-check counts, u, f1 and f2 on a 64^3 lattice to 1e-9, and the same
-    segmentation bit for bit (sign(phi - 0.5) of all 16.8 M voxels, its SHA-256)."""
+    residual-check counts; the sums and L2 norms of u, f1 and f2 to 1e-9; u, f1 and f2
+    on a 64^3 lattice to the fixture's float32 storage rounding (1e-7 relative L2); and
+    the same segmentation bit for bit (sign(phi - 0.5) of all 16.8 M voxels, its
+    SHA-256)."""
     fx, kw, u0, phi0 = _fixture_case(pkg)
     r = ctx.rsfe_apply(u0.astype(np.float64), phi0.astype(np.float64), pkg.default_params(**kw),
                        want_u=True, want_f=True)
@@ -88,8 +90,9 @@ def test_fp64_matches_the_reference_at_256(ctx, pkg):
     assert st["total_sweeps"] == int(fx["total_sweeps"])
     assert st["residual_checks"] == int(fx["residual_checks"])
     for key in ("u", "f1", "f2"):
-        assert rel(r[key][LATTICE], fx[key + "_lattice"].astype(np.float64)) <= 1e-9, key
+        assert rel(r[key][LATTICE], fx[key + "_lattice"].astype(np.float64)) <= 1e-7, key
         assert abs(float(r[key].sum()) - float(fx[key + "_sum"])) <= 1e-9 * abs(float(fx[key + "_sum"])), key
+        assert abs(float(np.linalg.norm(r[key])) - float(fx[key + "_l2"])) <= 1e-9 * float(fx[key + "_l2"]), key
     bits = np.packbits((r["phi"] > 0.5).ravel())
     assert hashlib.sha256(bits.tobytes()).hexdigest() == str(fx["inside_sha256"])
 
