@@ -123,22 +123,25 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-__device__ __forceinline__ long long block_linear_id()
+// Linear index and count of the blocks of a grid. The kernel bodies take their block
+// index and grid as arguments (a work-list launch over several volumes passes each
+// block's index within its own volume's grid), so these take them too.
+__device__ __forceinline__ long long block_linear_id(const uint3 b, const dim3 g)
 {
-    return blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    return b.x + (long long)g.x * (b.y + (long long)g.y * b.z);
 }
 
-__device__ __forceinline__ long long grid_blocks()
+__device__ __forceinline__ long long grid_blocks(const dim3 g)
 {
-    return (long long)gridDim.x * gridDim.y * gridDim.z;
+    return (long long)g.x * g.y * g.z;
 }
 
-// Block sums of one or two doubles, written by thread 0 to this block's slot of
-// `part` (part[b] and, for the second value, part[nblocks + b]). No atomics: a
-// one-block finalize kernel adds the slots in a fixed order, so the totals do not
-// depend on block scheduling.
+// Block sums of one or two doubles, written by thread 0 to block bid's slot of `part`
+// (part[bid] and, for the second value, part[nblocks + bid]). No atomics: a one-block
+// finalize kernel adds the slots in a fixed order, so the totals do not depend on
+// block scheduling.
 template <int NWARPS_MAX = 32>
-__device__ __forceinline__ void block_sum_store(double v, double* part)
+__device__ __forceinline__ void block_sum_store(double v, double* part, long long bid)
 {
     __shared__ double red_sm[NWARPS_MAX];
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -149,12 +152,13 @@ __device__ __forceinline__ void block_sum_store(double v, double* part)
     if (tid < 32) {
         double w = (tid < ((nthreads + 31) >> 5)) ? red_sm[tid] : 0.0;
         w = warp_sum(w);
-        if (tid == 0) part[block_linear_id()] = w;
+        if (tid == 0) part[bid] = w;
     }
 }
 
 template <int NWARPS_MAX = 32>
-__device__ __forceinline__ void block_sum2_store(double a, double b, double* part)
+__device__ __forceinline__ void block_sum2_store(double a, double b, double* part, long long bid,
+                                                 long long nblocks)
 {
     __shared__ double red_a[NWARPS_MAX], red_b[NWARPS_MAX];
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
@@ -173,9 +177,8 @@ __device__ __forceinline__ void block_sum2_store(double a, double b, double* par
         wa = warp_sum(wa);
         wb = warp_sum(wb);
         if (tid == 0) {
-            const long long bid = block_linear_id();
             part[bid] = wa;
-            part[grid_blocks() + bid] = wb;
+            part[nblocks + bid] = wb;
         }
     }
 }
@@ -185,9 +188,8 @@ __device__ __forceinline__ void block_sum2_store(double a, double b, double* par
 // four interleaved accumulators (m mod 4), so that four loads are in flight, then the
 // block adds the accumulators and the threads' sums in a fixed tree.
 constexpr int kFinThreads = 1024;
-static __global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const double* __restrict__ part,
-                                                                    long long nblocks, int nvals,
-                                                                    double* sums, int slot)
+__device__ __forceinline__ void finalize_sums_body(const double* __restrict__ part, long long nblocks,
+                                                   int nvals, double* sums, int slot)
 {
     __shared__ double sm[kFinThreads];
     for (int v = 0; v < nvals; ++v) {
@@ -212,6 +214,13 @@ static __global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const
         if (threadIdx.x == 0) sums[slot + v] = sm[0];
         __syncthreads();
     }
+}
+
+static __global__ void __launch_bounds__(kFinThreads) finalize_sums_kernel(const double* __restrict__ part,
+                                                                    long long nblocks, int nvals,
+                                                                    double* sums, int slot)
+{
+    finalize_sums_body(part, nblocks, nvals, sums, slot);
 }
 
 }  // namespace im3d

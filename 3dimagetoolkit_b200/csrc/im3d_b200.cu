@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "kernels.cuh"
+#include "worklist.cuh"
 
 using namespace im3d;
 
@@ -64,6 +65,13 @@ struct im3d_ctx {
     std::vector<std::pair<std::string, Acc>> prof_acc;
     // worker contexts of the batched entry points (own stream and buffers each)
     std::vector<im3d_ctx*> workers;
+    // per-volume contexts of a work-list batch (buffers and control block of each
+    // volume; their launches go to this context's stream), and the group's pinned
+    // control blocks
+    std::vector<im3d_ctx*> vols;
+    Ctrl* wl_ctrl_h = nullptr;
+    int wl_ctrl_cap = 0;
+    int batch_mode = IM3D_BATCH_AUTO;
     int num_sms = 148;
     int ifit_chunks = 0;  // i chunks of the marching fit stage (0: cost model)
     size_t mem_limit = 0;  // device bytes the context may hold in buffers (0: no limit)
@@ -382,15 +390,24 @@ int set_smem(im3d_ctx* ctx, K kernel, size_t bytes)
     return IM3D_OK;
 }
 
+// Register-window k pass: blocks of RKR rows x TKT threads, 4 outputs per thread.
+constexpr int kKwT = 32, kKwR = 8;
+template <typename T, int N, int S>
+constexpr size_t k_win_smem() { return (size_t)N * kKwR * (kKwT * 4 + 2 * ((S + 3) & ~3)) * sizeof(T); }
+dim3 k_win_grid(const Dims& d)
+{
+    const long long rows = (long long)d.nx * d.ny;
+    return dim3((unsigned)((rows + kKwR - 1) / kKwR), (d.nz + kKwT * 4 - 1) / (kKwT * 4));
+}
+
 template <typename T, int N, int S, class Ld, class St>
 int pass_k_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const char* name)
 {
-    constexpr int TKT = 32, RKR = 8, TKW = TKT * 4, SP = (S + 3) & ~3;
-    const size_t smem = (size_t)N * RKR * (TKW + 2 * SP) * sizeof(T);
+    constexpr int TKT = kKwT, RKR = kKwR;
+    const size_t smem = k_win_smem<T, N, S>();
     auto kern = conv_k_win_kernel<T, N, S, TKT, RKR, Ld, St>;
     IM3D_TRY(set_smem(ctx, kern, smem));
-    const long long rows = (long long)d.nx * d.ny;
-    dim3 grid((unsigned)((rows + RKR - 1) / RKR), (d.nz + TKW - 1) / TKW);
+    const dim3 grid = k_win_grid(d);
     const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TKT, RKR), smem, ctx->stream>>>(ld, st, d, w);
     prof_end(ctx, pf);
@@ -415,17 +432,27 @@ int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
     return check_launch(ctx, name);
 }
 
+// Register-window j / i pass: TW x TY blocks, R outputs per thread along the axis.
+template <typename T> struct SWinR { static constexpr int v = sizeof(T) == 4 ? 8 : 4; };
+template <typename T, int N, int S>
+constexpr size_t s_win_smem() { return (size_t)N * (TY * SWinR<T>::v + 2 * S) * TW * sizeof(T); }
+template <typename T, int AXIS>
+dim3 s_win_grid(const Dims& d)
+{
+    constexpr int TA = TY * SWinR<T>::v;
+    const int len = AXIS == 0 ? d.nx : d.ny;
+    const int other = AXIS == 0 ? d.ny : d.nx;
+    return dim3((d.nz + TW - 1) / TW, (len + TA - 1) / TA, other);
+}
+
 template <typename T, int N, int AXIS, int S, class Ld, class St>
 int pass_s_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const char* name)
 {
-    constexpr int R = sizeof(T) == 4 ? 8 : 4;
-    constexpr int TA = TY * R;
-    const size_t smem = (size_t)N * (TA + 2 * S) * TW * sizeof(T);
+    constexpr int R = SWinR<T>::v;
+    const size_t smem = s_win_smem<T, N, S>();
     auto kern = conv_s_win_kernel<T, N, AXIS, S, TW, TY, R, Ld, St>;
     IM3D_TRY(set_smem(ctx, kern, smem));
-    const int len = AXIS == 0 ? d.nx : d.ny;
-    const int other = AXIS == 0 ? d.ny : d.nx;
-    dim3 grid((d.nz + TW - 1) / TW, (len + TA - 1) / TA, other);
+    const dim3 grid = s_win_grid<T, AXIS>(d);
     const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w);
     prof_end(ctx, pf);
@@ -453,16 +480,28 @@ int pass_s(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
 }
 
 template <typename T, int S>
-int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T* f2,
-                   const Dims& d, const T* w, T l1, T l2)
+constexpr size_t fit_win_smem()
 {
     constexpr int TA = TileA<T>::v;
     constexpr int RA = (TA + 2 * S + TY - 1) / TY;
     constexpr int H2 = TY * RA, H1 = H2 + 2 * S;
-    const size_t smem = (size_t)(4 * H1 + 2 * H2) * TW * sizeof(T);
+    return (size_t)(4 * H1 + 2 * H2) * TW * sizeof(T);
+}
+template <typename T>
+dim3 fit_win_grid(const Dims& d)
+{
+    return dim3((d.nz + TW - 1) / TW, (d.nx + TileA<T>::v - 1) / TileA<T>::v, d.ny);
+}
+
+template <typename T, int S>
+int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T* f2,
+                   const Dims& d, const T* w, T l1, T l2)
+{
+    constexpr int TA = TileA<T>::v;
+    const size_t smem = fit_win_smem<T, S>();
     auto kern = conv_i_fit_win_kernel<T, S, TW, TY, TA>;
     IM3D_TRY(set_smem(ctx, kern, smem));
-    dim3 grid((d.nz + TW - 1) / TW, (d.nx + TA - 1) / TA, d.ny);
+    const dim3 grid = fit_win_grid<T>(d);
     const int pf = prof_begin(ctx, "conv_i_fit");
     kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(in, out, f1, f2, d, w, l1, l2);
     prof_end(ctx, pf);
@@ -474,14 +513,16 @@ int pass_i_fit_win(im3d_ctx* ctx, const Vec<T, 4>* in, Vec<T, 2>* out, T* f1, T*
 // ceil(blocks / SMs) x (chunk + 4S), where each chunk re-streams 4S halo planes
 // (measured at 256^3: 1, 2, 3, 4 chunks take 152, 144, 160, 164 us; this picks 2).
 // The context option IM3D_OPT_FIT_CHUNKS overrides it.
+// 4 blocks of 128 threads per SM for 19 taps (126 registers, no spills); 2 for 25
+// taps (3 would spill)
+constexpr int kMarchJB = 4, kMarchD = 16, kMarchU = 4;
+template <int S> struct MarchMinB { static constexpr int v = S <= 9 ? 4 : 2; };
+
+// planes of i per block of the marching i-stage, and its grid
 template <int S>
-int pass_i_fit_march(im3d_ctx* ctx, const Vec<float, 4>* in, Vec<float, 2>* out, float* f1,
-                     float* f2, const Dims& d, const float* hw, float l1, float l2)
+int march_chunk(const im3d_ctx* ctx, const Dims& d, dim3* grid)
 {
-    // 4 blocks of 128 threads per SM for 19 taps (126 registers, no spills); 2 for 25
-    // taps (3 would spill)
-    constexpr int JB = 4, D = 16, U = 4, MINB = S <= 9 ? 4 : 2;
-    auto kern = conv_i_fit_march_kernel<S, JB, D, U, MINB>;
+    constexpr int JB = kMarchJB;
     const long long cols = (long long)((d.nz + 31) / 32) * ((d.ny + JB - 1) / JB);
     int chunks = ctx->ifit_chunks;
     if (chunks <= 0) {
@@ -498,9 +539,27 @@ int pass_i_fit_march(im3d_ctx* ctx, const Vec<float, 4>* in, Vec<float, 2>* out,
     }
     chunks = std::min(chunks, d.nx);
     const int chunk = (d.nx + chunks - 1) / chunks;
-    dim3 grid((d.nz + 31) / 32, (d.ny + JB - 1) / JB, (d.nx + chunk - 1) / chunk);
+    *grid = dim3((d.nz + 31) / 32, (d.ny + JB - 1) / JB, (d.nx + chunk - 1) / chunk);
+    return chunk;
+}
+
+template <int S>
+TapPairs<S> tap_pairs(const float* hw)
+{
     TapPairs<S> tp;
     for (int t = 0; t <= S; ++t) tp.w[t] = make_float2(hw[t], hw[t]);
+    return tp;
+}
+
+template <int S>
+int pass_i_fit_march(im3d_ctx* ctx, const Vec<float, 4>* in, Vec<float, 2>* out, float* f1,
+                     float* f2, const Dims& d, const float* hw, float l1, float l2)
+{
+    constexpr int JB = kMarchJB, D = kMarchD, U = kMarchU, MINB = MarchMinB<S>::v;
+    auto kern = conv_i_fit_march_kernel<S, JB, D, U, MINB>;
+    dim3 grid;
+    const int chunk = march_chunk<S>(ctx, d, &grid);
+    const TapPairs<S> tp = tap_pairs<S>(hw);
     const int pf = prof_begin(ctx, "conv_i_fit");
     kern<<<grid, dim3(32, JB), 0, ctx->stream>>>(reinterpret_cast<const float4*>(in),
                                                  reinterpret_cast<float2*>(out), f1, f2, d, tp,
@@ -965,10 +1024,11 @@ int ws_status(im3d_ctx* ctx, int st)
 }
 
 // Before a solve: IM3D_WS_PREDICT adds the network's correction to u_in when that
-// lowers the residual; both modes keep u_in in w.upk0.
-int ws_before(im3d_ctx* ctx, const Dims& d, const GsCoef<float>& c, float* upk, const float* bpk,
-              const float* prevu, const float* divdb, const float* phi, float inv_dt, int dirichlet,
-              const WsBufs& w, int* used, int* rejected)
+// lowers the residual; both modes keep u_in in w.upk0. (FP32 entry points only.)
+[[maybe_unused]] int ws_before(im3d_ctx* ctx, const Dims& d, const GsCoef<float>& c, float* upk,
+                               const float* bpk, const float* prevu, const float* divdb,
+                               const float* phi, float inv_dt, int dirichlet, const WsBufs& w,
+                               int* used, int* rejected)
 {
     ws_fields_kernel<<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(bpk, upk, prevu, divdb, phi, d, inv_dt, w.x);
     IM3D_TRY(check_launch(ctx, "ws_fields"));
@@ -997,8 +1057,9 @@ int ws_before(im3d_ctx* ctx, const Dims& d, const GsCoef<float>& c, float* upk, 
 }
 
 // After a solve (IM3D_WS_TRAIN): one training step on the solve's fields and the
-// correction it made.
-int ws_after(im3d_ctx* ctx, const Dims& d, const float* upk, const WsBufs& w, double* loss)
+// correction it made. (FP32 entry points only.)
+[[maybe_unused]] int ws_after(im3d_ctx* ctx, const Dims& d, const float* upk, const WsBufs& w,
+                              double* loss)
 {
     ws_target_kernel<<<grid_vol(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(upk, w.upk0, d, w.y);
     IM3D_TRY(check_launch(ctx, "ws_target"));
@@ -1012,23 +1073,9 @@ int ws_after(im3d_ctx* ctx, const Dims& d, const float* upk, const WsBufs& w, do
 }
 
 // --------------------------------------------------------------- the loop
-template <typename T>
-struct Outs {
-    T* phi;
-    T* u;
-    T* f1;
-    T* f2;
-};
-
-template <typename T>
-int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, int ny, int nz,
-               double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
-               T* f1_user, T* f2_user, im3d_rsfe_stats* stats)
+// The setters' checks (rsfe_splitbregman_imp.hxx:806-1440), with their WARNING texts.
+int check_params(im3d_ctx* ctx, const im3d_rsfe_params* p)
 {
-    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
-    if (!p) return fail(ctx, IM3D_ERR_INVALID_ARG, "params must not be NULL");
-    if (!myim_user || !phi_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "myim and phi_out are required");
-    // the setters' checks (rsfe_splitbregman_imp.hxx:806-1440)
     if (!(p->sigma > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_sigma: sigma must be greater than zero");
     if (!(p->lamda > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_lamda: lamda must be greater than zero");
     if (!(p->lamda1 > 0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "WARNING::set_lamda1: lamda1 must be greater than zero");
@@ -1046,22 +1093,43 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     if (!(p->b0 > p->a0)) return fail(ctx, IM3D_ERR_INVALID_ARG, "b0 has to be greater than a0");
     if (p->gs_rel_res_tol > 0 && !(p->omega > 0 && p->omega < 2))
         return fail(ctx, IM3D_ERR_INVALID_ARG, "omega must lie in (0, 2)");
-    const bool ws = ctx->ws_net && ctx->ws_mode != IM3D_WS_OFF && p->gs_rel_res_tol > 0;
-    if (ws && !std::is_same<T, float>::value)
-        return fail(ctx, IM3D_ERR_UNSUPPORTED, "the learned warm start runs with the FP32 entry point");
+    return IM3D_OK;
+}
 
-    // a pending resume is consumed by this call, whatever its outcome
-    const bool resuming = ctx->resume;
-    const im3d_rsfe_checkpoint from = ctx->resume_from;
-    ctx->resume = false;
-    if (resuming) {
-        if (ctx->resume_esize != (int)sizeof(T))
-            return fail(ctx, IM3D_ERR_INVALID_ARG, "the checkpoint's element size does not match this call");
-        if (!from.phi || !from.b || !from.divdb || from.t < 0)
-            return fail(ctx, IM3D_ERR_INVALID_ARG, "a checkpoint needs phi, b, divdb and t >= 0");
-    }
+// One volume's device state and loop counters (rsfe_prepare fills it).
+template <typename T>
+struct VolState {
+    Dims d;
+    long long n = 0, npk2 = 0;
+    double chosen_bc = 0, hhh = 1;
+    T a0 = 0, b0 = 1, center = 0, inv_eps = 0;
+    const T* u0 = nullptr;
+    T *phi = nullptr, *other = nullptr, *g = nullptr, *divdb = nullptr, *b3 = nullptr, *dmb = nullptr,
+      *kones = nullptr, *rhs = nullptr, *upk = nullptr, *bpk = nullptr, *prev = nullptr;
+    Vec<T, 4>*W1 = nullptr, *W2 = nullptr;
+    Vec<T, 2>*P1 = nullptr, *P2 = nullptr;
+    T *u_d = nullptr, *f1_d = nullptr, *f2_d = nullptr;
+    Taps<T> tp;
+    GsCoef<T> coef;
+    int t0 = 0;  // outer iterations already done (a resumed run)
+    double tollerance = 1000;
+    int init_variables = 0;
+    int sched_first = 0;  // residual schedule carried between Poisson solves
+    double sched_rate = 0;
+};
 
-    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+// Everything before the outer loop of rsfe_splitbregman<T>::apply for one volume, on
+// the context's stream and in its buffers: inputs, the refusal of non-finite values,
+// the initial level set (or a checkpoint's state), taps, kones and the edge detector
+// (rsfe_splitbregman_imp.hxx:1547-1660). `from` resumes from a checkpoint; `wsb`
+// receives the learned warm start's buffers.
+template <typename T>
+int rsfe_prepare(im3d_ctx* ctx, VolState<T>& v, const T* myim_user, const T* init_user, int nx,
+                 int ny, int nz, double hx, double hy, double hz, const im3d_rsfe_params* p,
+                 T* u_user, T* f1_user, T* f2_user, const im3d_rsfe_checkpoint* from, WsBufs* wsb)
+{
+    const bool resuming = from != nullptr;
+    const bool ws = wsb != nullptr;
     // the convolution passes take the plug-in's boundary; no other kernel reads cyc
     Dims d{nx, ny, nz};
     d.cyc = p->conv_cyclic ? 1 : 0;
@@ -1106,13 +1174,10 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     IM3D_TRY(dev_out<T>(ctx, f2_user, n, "out_f2", &f2_d));
     if (f1_d && !f2_d) IM3D_TRY(tbuf<T>(ctx, "out_f2", n, &f2_d));
     if (f2_d && !f1_d) IM3D_TRY(tbuf<T>(ctx, "out_f1", n, &f1_d));
-    WsBufs wsb{nullptr, nullptr, nullptr};
-    int ws_used = 0, ws_rejected = 0, ws_steps = 0;
-    double ws_loss = 0;
     if (ws) {
-        IM3D_TRY(tbuf<float>(ctx, "ws_x", 4 * (size_t)n, &wsb.x));
-        IM3D_TRY(tbuf<float>(ctx, "ws_y", (size_t)n, &wsb.y));
-        IM3D_TRY(tbuf<float>(ctx, "ws_upk0", (size_t)npk2, &wsb.upk0));
+        IM3D_TRY(tbuf<float>(ctx, "ws_x", 4 * (size_t)n, &wsb->x));
+        IM3D_TRY(tbuf<float>(ctx, "ws_y", (size_t)n, &wsb->y));
+        IM3D_TRY(tbuf<float>(ctx, "ws_upk0", (size_t)npk2, &wsb->upk0));
         // the previous solve's u: the clamp kernel writes it (before the clamp)
         if (!u_d) IM3D_TRY(tbuf<T>(ctx, "ws_prevu", n, &u_d));
     }
@@ -1133,14 +1198,14 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
     double sched_rate = 0;
     if (resuming) {
         // the state of the checkpoint instead of the initial level set
-        IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, from.phi, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
-        IM3D_CUDA(ctx, cudaMemcpyAsync(b3, from.b, 3 * n * sizeof(T), cudaMemcpyDefault, ctx->stream));
-        IM3D_CUDA(ctx, cudaMemcpyAsync(divdb, from.divdb, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
-        t0 = from.t;
-        tollerance = from.tollerance;
-        init_variables = from.init_variables;
-        sched_first = from.sched_first;
-        sched_rate = from.sched_rate;
+        IM3D_CUDA(ctx, cudaMemcpyAsync(phiA, from->phi, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(b3, from->b, 3 * n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(divdb, from->divdb, n * sizeof(T), cudaMemcpyDefault, ctx->stream));
+        t0 = from->t;
+        tollerance = from->tollerance;
+        init_variables = from->init_variables;
+        sched_first = from->sched_first;
+        sched_rate = from->sched_rate;
     } else {
         // initial level set (rsfe_splitbregman_imp.hxx:99-170 / :48-95), then
         // change_range_of_intensity(b0, a0) (image3d_imp.hxx:1628-1636)
@@ -1184,18 +1249,115 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             src, g, d, hx, hy, hz, (T)p->beta, (T)p->lamda, (T)p->nu);
         IM3D_TRY(check_launch(ctx, "edge"));
     }
-    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
 
-    const GsCoef<T> coef = make_coef<T>(hx, hy, hz, p->dt, chosen_bc, neu ? 1 : 0);
-    const T center = (T)((p->a0 + p->b0) / 2.);
-    const T inv_eps = (T)(1.0 / p->epsilon);
-    const double hhh = hx * hy * hz;
+    v.d = d;
+    v.n = n;
+    v.npk2 = npk2;
+    v.chosen_bc = chosen_bc;
+    v.hhh = hx * hy * hz;
+    v.a0 = a0;
+    v.b0 = b0;
+    v.center = (T)((p->a0 + p->b0) / 2.);
+    v.inv_eps = (T)(1.0 / p->epsilon);
+    v.u0 = u0;
+    v.phi = phiA;
+    v.other = phiB;
+    v.g = g;
+    v.divdb = divdb;
+    v.b3 = b3;
+    v.dmb = dmb;
+    v.kones = kones;
+    v.rhs = rhs;
+    v.upk = upk;
+    v.bpk = bpk;
+    v.prev = prev;
+    v.W1 = W1;
+    v.W2 = W2;
+    v.P1 = P1;
+    v.P2 = P2;
+    v.u_d = u_d;
+    v.f1_d = f1_d;
+    v.f2_d = f2_d;
+    v.tp = tp;
+    v.coef = make_coef<T>(hx, hy, hz, p->dt, chosen_bc, neu ? 1 : 0);
+    v.t0 = t0;
+    v.tollerance = tollerance;
+    v.init_variables = init_variables;
+    v.sched_first = sched_first;
+    v.sched_rate = sched_rate;
+    return IM3D_OK;
+}
+
+template <typename T>
+struct Outs {
+    T* phi;
+    T* u;
+    T* f1;
+    T* f2;
+};
+
+template <typename T>
+int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, int ny, int nz,
+               double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
+               T* f1_user, T* f2_user, im3d_rsfe_stats* stats)
+{
+    IM3D_TRY(check_dims(ctx, nx, ny, nz, hx, hy, hz));
+    if (!p) return fail(ctx, IM3D_ERR_INVALID_ARG, "params must not be NULL");
+    if (!myim_user || !phi_user) return fail(ctx, IM3D_ERR_INVALID_ARG, "myim and phi_out are required");
+    IM3D_TRY(check_params(ctx, p));
+    const bool ws = ctx->ws_net && ctx->ws_mode != IM3D_WS_OFF && p->gs_rel_res_tol > 0;
+    if (ws && !std::is_same<T, float>::value)
+        return fail(ctx, IM3D_ERR_UNSUPPORTED, "the learned warm start runs with the FP32 entry point");
+
+    // a pending resume is consumed by this call, whatever its outcome
+    const bool resuming = ctx->resume;
+    const im3d_rsfe_checkpoint from = ctx->resume_from;
+    ctx->resume = false;
+    if (resuming) {
+        if (ctx->resume_esize != (int)sizeof(T))
+            return fail(ctx, IM3D_ERR_INVALID_ARG, "the checkpoint's element size does not match this call");
+        if (!from.phi || !from.b || !from.divdb || from.t < 0)
+            return fail(ctx, IM3D_ERR_INVALID_ARG, "a checkpoint needs phi, b, divdb and t >= 0");
+    }
+
+    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    const bool solve = p->gs_rel_res_tol > 0;
+    const bool lex = !solve && p->sweep == IM3D_SWEEP_LEXICOGRAPHIC;
+    const bool neu = p->bc == IM3D_BC_NEU;
+    VolState<T> vs;
+    WsBufs wsb{nullptr, nullptr, nullptr};
+    IM3D_TRY(rsfe_prepare<T>(ctx, vs, myim_user, init_user, nx, ny, nz, hx, hy, hz, p, u_user, f1_user,
+                             f2_user, resuming ? &from : nullptr, ws ? &wsb : nullptr));
+    IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    const Dims d = vs.d;
+    const long long n = vs.n;
+    const long long npk2 = vs.npk2;
+    const double chosen_bc = vs.chosen_bc;
+    const T a0 = vs.a0, b0 = vs.b0;
+    const T* u0 = vs.u0;
+    T *g = vs.g, *divdb = vs.divdb, *b3 = vs.b3, *dmb = vs.dmb, *kones = vs.kones, *rhs = vs.rhs,
+      *upk = vs.upk, *bpk = vs.bpk, *prev = vs.prev;
+    Vec<T, 4>*W1 = vs.W1, *W2 = vs.W2;
+    Vec<T, 2>*P1 = vs.P1, *P2 = vs.P2;
+    T *u_d = vs.u_d, *f1_d = vs.f1_d, *f2_d = vs.f2_d;
+    const Taps<T>& tp = vs.tp;
+    const GsCoef<T> coef = vs.coef;
+    const T center = vs.center;
+    const T inv_eps = vs.inv_eps;
+    const double hhh = vs.hhh;
+    const int t0 = vs.t0;
+    double tollerance = vs.tollerance;
+    int init_variables = vs.init_variables;
+    int sched_first = vs.sched_first;
+    double sched_rate = vs.sched_rate;
+    int ws_used = 0, ws_rejected = 0, ws_steps = 0;
+    double ws_loss = 0;
     long long total_sweeps = 0;
     int last_sweeps = 0, not_conv = 0, t;
     const long long checks0 = ctx->residual_checks;
     double last_rel = -1, last_ls_err = -1;
-    T* phi = phiA;   // current level set (natural)
-    T* other = phiB;
+    T* phi = vs.phi;  // current level set (natural)
+    T* other = vs.other;
 
     for (t = t0 + 1; tollerance > p->tol && t <= p->maxiter; ++t) {
         // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
@@ -1758,6 +1920,484 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
                T* f1_user, T* f2_user, im3d_rsfe_stats* stats);
 
+// ------------------------------------------------------------ work-list batch
+// Volumes of a group advance their outer iterations together; each stage of the loop
+// is one launch over every volume that runs it (worklist.cuh).
+
+template <class Job>
+struct JobTable {
+    std::vector<JobSlot<Job>> h;
+    JobSlot<Job>* d = nullptr;
+};
+
+template <class Job>
+int upload_jobs(im3d_ctx* ctx, const char* name, JobTable<Job>& t)
+{
+    IM3D_TRY(tbuf<JobSlot<Job>>(ctx, name, t.h.size(), &t.d));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(t.d, t.h.data(), t.h.size() * sizeof(JobSlot<Job>),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    return IM3D_OK;
+}
+
+WorkList make_worklist(const std::vector<int>& sel, const int* flags)
+{
+    WorkList wl;
+    wl.n = (int)sel.size();
+    for (int e = 0; e < wl.n; ++e) {
+        wl.vol[e] = sel[e];
+        wl.flag[e] = flags ? flags[e] : 0;
+    }
+    return wl;
+}
+
+// One launch of a stage over the volumes `sel` (indices into the job table).
+template <class Job, int THREADS, int MINB>
+int wl_launch(im3d_ctx* ctx, const JobTable<Job>& t, const std::vector<int>& sel, const int* flags,
+              dim3 blk, size_t smem, const char* name, bool dependent = false)
+{
+    if (sel.empty()) return IM3D_OK;
+    WorkList wl = make_worklist(sel, flags);
+    long long total = 0;
+    for (int e = 0; e < wl.n; ++e) {
+        const dim3 g = t.h[sel[e]].grid;
+        wl.first[e] = total;
+        total += (long long)g.x * g.y * g.z;
+    }
+    wl.first[wl.n] = total;
+    if (total > 0x7fffffffLL) return fail(ctx, IM3D_ERR_INVALID_ARG, "work list too large for one launch");
+    auto kern = worklist_kernel<Job, THREADS, MINB>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    const int pf = prof_begin(ctx, name);
+    if (dependent) IM3D_TRY(launch_dependent(ctx, kern, dim3((unsigned)total), blk, t.d, wl));
+    else kern<<<dim3((unsigned)total), blk, smem, ctx->stream>>>(t.d, wl);
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
+}
+
+// The partials of the last reduction of `sel` folded into each volume's control block.
+int wl_finalize(im3d_ctx* ctx, const FinalizeJob* jobs, const std::vector<int>& sel, const int* flags,
+                int nvals, int slot)
+{
+    if (sel.empty()) return IM3D_OK;
+    const WorkList wl = make_worklist(sel, flags);
+    finalize_worklist_kernel<<<wl.n, kFinThreads, 0, ctx->stream>>>(jobs, wl, nvals, slot);
+    return check_launch(ctx, "finalize_sums");
+}
+
+// Whether a batch can run as a work list (the volumes were checked by check_dims).
+template <typename T>
+bool worklist_eligible(const im3d_rsfe_params* p, int nvol, const im3d_volume_desc* vols, int* nh_out)
+{
+    if (!(p->gs_rel_res_tol > 0) || p->omega != 1.0 || p->auto_extract_conn_comp || p->conv_cyclic)
+        return false;
+    int nh0 = 0;
+    for (int v = 0; v < nvol; ++v) {
+        std::vector<double> w;
+        const double hs[3] = {p->gaussian_pixel_approach ? 1. : vols[v].hx,
+                              p->gaussian_pixel_approach ? 1. : vols[v].hy,
+                              p->gaussian_pixel_approach ? 1. : vols[v].hz};
+        for (int a = 0; a < 3; ++a) {
+            const int nh = gauss_taps_host(p->sigma, 3.0, hs[a], w);
+            if (nh != 19 && nh != 25) return false;
+            if (nh0 == 0) nh0 = nh;
+            if (nh != nh0) return false;
+        }
+    }
+    *nh_out = nh0;
+    return true;
+}
+
+// Per-volume loop counters of a work-list group.
+struct WlCount {
+    bool done = false;
+    long long total_sweeps = 0;
+    int last_sweeps = 0, not_conv = 0, checks = 0, iterations = 0;
+    double last_rel = -1;
+    // the current Poisson solve (rb_solve's state)
+    int s = 0, s_prev = 0, next = 0;
+    double r_prev = -1, rate_used = 0, beff2 = -1, rel = -1;
+    bool conv = false;
+};
+
+template <typename T, int S>
+int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume_desc* vols,
+                   const im3d_rsfe_params* p, im3d_rsfe_stats* stats, double* latency_ms,
+                   std::chrono::steady_clock::time_point t_start)
+{
+    const int nv = (int)ids.size();
+    const bool neu = p->bc == IM3D_BC_NEU;
+    while ((int)ctx->vols.size() < nv) {
+        im3d_ctx* v = nullptr;
+        const int st = im3d_ctx_create(ctx->device, &v);
+        if (st != IM3D_OK) return fail(ctx, st, "cannot create a volume context");
+        ctx->vols.push_back(v);
+    }
+    if (ctx->wl_ctrl_cap < nv) {
+        if (ctx->wl_ctrl_h) cudaFreeHost(ctx->wl_ctrl_h);
+        ctx->wl_ctrl_h = nullptr;
+        ctx->wl_ctrl_cap = 0;
+        IM3D_CUDA(ctx, cudaMallocHost(&ctx->wl_ctrl_h, kMaxListVols * sizeof(Ctrl)));
+        ctx->wl_ctrl_cap = kMaxListVols;
+    }
+    Ctrl* ctrl = nullptr;
+    IM3D_TRY(tbuf<Ctrl>(ctx, "wl_ctrl", kMaxListVols, &ctrl, true));
+
+    // set-up of every volume (its own buffers, on this stream); the device-memory
+    // budget of the context covers the group as a whole
+    std::vector<VolState<T>> V(nv);
+    std::vector<double*> part_res(nv), part_cl(nv);
+    for (int q = 0; q < nv; ++q) {
+        im3d_ctx* vc = ctx->vols[q];
+        vc->stream = ctx->stream;
+        vc->ifit_chunks = ctx->ifit_chunks;
+        vc->prof = 0;
+        vc->err.clear();
+        if (ctx->mem_limit) {
+            size_t others = ctx->mem_held;
+            for (int r = 0; r < (int)ctx->vols.size(); ++r)
+                if (r != q) others += ctx->vols[r]->mem_held;
+            vc->mem_limit = ctx->mem_limit > others ? ctx->mem_limit - others : 1;
+        } else {
+            vc->mem_limit = 0;
+        }
+        const im3d_volume_desc& dsc = vols[ids[q]];
+        int st = rsfe_prepare<T>(vc, V[q], static_cast<const T*>(dsc.myim), static_cast<const T*>(dsc.init),
+                                 dsc.nx, dsc.ny, dsc.nz, dsc.hx, dsc.hy, dsc.hz, p, nullptr, nullptr,
+                                 nullptr, nullptr, nullptr);
+        const Dims& d = V[q].d;
+        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2);
+        const bool vec = d.nz % V16<T>::W == 0;
+        const dim3 gc = vec ? grid_vec<T>(d, kBlkVec) : grid_col(d, kBlkVol);
+        if (st == IM3D_OK)
+            st = tbuf<double>(vc, "wl_part_res", 2 * (size_t)gr.x * gr.y * gr.z, &part_res[q]);
+        if (st == IM3D_OK)
+            st = tbuf<double>(vc, "wl_part_clamp", 2 * (size_t)gc.x * gc.y * gc.z, &part_cl[q]);
+        if (st != IM3D_OK) return fail(ctx, st, "volume " + std::to_string(ids[q]) + ": " + vc->err);
+    }
+
+    // job tables: every stage's arguments and grid, per volume
+    constexpr int R = SWinR<T>::v;
+    using KHeav = ConvKWinJob<T, 4, S, kKwT, kKwR, LdHeaviside<T>, StVec<T, 4>>;
+    using SJ4 = ConvSWinJob<T, 4, 1, S, TW, TY, R, LdVec<T, 4>, StVec<T, 4>>;
+    using SJ2 = ConvSWinJob<T, 2, 1, S, TW, TY, R, LdVec<T, 2>, StVec<T, 2>>;
+    using KRhs = ConvKWinJob<T, 2, S, kKwT, kKwR, LdVec<T, 2>, StRhs<T>>;
+    using FitM = FitMarchJob<S, kMarchJB, kMarchD, kMarchU, MarchMinB<S>::v>;
+    using FitW = FitWinJob<T, S, TW, TY, TileA<T>::v>;
+    constexpr int RB_MINB = sizeof(T) == 4 ? 8 : 1;
+    using RbD = RbHalfJob<T, kNV, false, RB_MINB>;
+    using RbN = RbHalfJob<T, kNV, true, 1>;
+    using Res = RbResidualJob<T, kNV>;
+    using ClV = ClampTolJob<T, kNV, true>;
+    using ClS = ClampTolJob<T, kNI, false>;
+    using BrV = BregmanJob<T, kNV, true>;
+    using BrS = BregmanJob<T, kNI, false>;
+    using DvV = DivJob<T, kNV, true>;
+    using DvS = DivJob<T, 0, false>;
+    JobTable<KHeav> jk;
+    JobTable<SJ4> js4;
+    JobTable<SJ2> js2;
+    JobTable<KRhs> jr;
+    JobTable<FitM> jfm;
+    JobTable<FitW> jfw;
+    JobTable<RbD> jrd[2];
+    JobTable<RbN> jrn[2];
+    JobTable<Res> jres;
+    JobTable<ClV> jclv;
+    JobTable<ClS> jcls;
+    JobTable<BrV> jbrv;
+    JobTable<BrS> jbrs;
+    JobTable<DvV> jdvv;
+    JobTable<DvS> jdvs;
+    std::vector<FinalizeJob> fin_res(nv), fin_cl(nv);
+    std::vector<char> vecrow(nv);
+    const T l1 = (T)p->lamda1, l2 = (T)p->lamda2;
+    for (int q = 0; q < nv; ++q) {
+        const VolState<T>& v = V[q];
+        const Dims& d = v.d;
+        const double hx = vols[ids[q]].hx, hy = vols[ids[q]].hy, hz = vols[ids[q]].hz;
+        jk.h.push_back({KHeav{LdHeaviside<T>{v.phi, v.u0, d, v.center, v.inv_eps}, StVec<T, 4>{v.W1, d}, d,
+                              v.tp.w[2]}, k_win_grid(d)});
+        js4.h.push_back({SJ4{LdVec<T, 4>{v.W1, d}, StVec<T, 4>{v.W2, d}, d, v.tp.w[1]}, s_win_grid<T, 1>(d)});
+        js2.h.push_back({SJ2{LdVec<T, 2>{v.P1, d}, StVec<T, 2>{v.P2, d}, d, v.tp.w[1]}, s_win_grid<T, 1>(d)});
+        StRhs<T> st;
+        st.u0 = v.u0; st.kones = v.kones; st.divdb = v.divdb; st.phi = v.phi;
+        st.out = v.bpk;
+        st.upk = v.upk;
+        st.beff2 = nullptr;
+        st.d = d;
+        st.l12 = (T)(p->lamda1 - p->lamda2);
+        st.lamda = (T)p->lamda;
+        st.inv_lamda = (T)(1.0 / p->lamda);
+        st.inv_dt = (T)(1.0 / p->dt);
+        st.bc = (T)v.chosen_bc;
+        st.mode = 2;
+        st.dirichlet = neu ? 0 : 1;
+        jr.h.push_back({KRhs{LdVec<T, 2>{v.P2, d}, st, d, v.tp.w[2]}, k_win_grid(d)});
+        if constexpr (sizeof(T) == 4) {
+            dim3 g;
+            const int chunk = march_chunk<S>(ctx->vols[q], d, &g);
+            jfm.h.push_back({FitM{reinterpret_cast<const float4*>(v.W2), reinterpret_cast<float2*>(v.P1),
+                                  v.f1_d, v.f2_d, d, tap_pairs<S>(v.tp.host[0]), l1, l2, chunk}, g});
+        } else {
+            jfw.h.push_back({FitW{v.W2, v.P1, v.f1_d, v.f2_d, d, v.tp.w[0], l1, l2}, fit_win_grid<T>(d)});
+        }
+        const dim3 gpk = grid_vec_pk<T>(d, kBlkVec);
+        for (int c = 0; c < 2; ++c) {
+            // red walks the planes forward, black backward (rb_sweep)
+            jrd[c].h.push_back({RbD{v.upk, v.bpk, d, v.coef, c, c}, gpk});
+            jrn[c].h.push_back({RbN{v.upk, v.bpk, d, v.coef, c, c}, gpk});
+        }
+        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2);
+        jres.h.push_back({Res{v.upk, v.bpk, d, v.coef, part_res[q]}, gr});
+        fin_res[q] = FinalizeJob{part_res[q], (long long)gr.x * gr.y * gr.z, ctrl[q].sum};
+        vecrow[q] = d.nz % V16<T>::W == 0;
+        const dim3 gv = grid_vec<T>(d, kBlkVec), gcol = grid_col(d, kBlkVol), gvol = grid_vol(d, kBlkVol);
+        jclv.h.push_back({ClV{v.upk, v.phi, nullptr, d, v.a0, v.b0, part_cl[q]}, gv});
+        jcls.h.push_back({ClS{v.upk, v.phi, nullptr, d, v.a0, v.b0, part_cl[q]}, gcol});
+        const dim3 gcl = vecrow[q] ? gv : gcol;
+        fin_cl[q] = FinalizeJob{part_cl[q], (long long)gcl.x * gcl.y * gcl.z, ctrl[q].sum};
+        jbrv.h.push_back({BrV{v.phi, v.b3, v.dmb, v.g, d, hx, hy, hz}, gv});
+        jbrs.h.push_back({BrS{v.phi, v.b3, v.dmb, v.g, d, hx, hy, hz}, gcol});
+        jdvv.h.push_back({DvV{v.dmb, v.divdb, d, hx, hy, hz}, gv});
+        jdvs.h.push_back({DvS{v.dmb, v.divdb, d, hx, hy, hz}, gvol});
+    }
+    IM3D_TRY(upload_jobs(ctx, "wl_k_heaviside", jk));
+    IM3D_TRY(upload_jobs(ctx, "wl_s_j4", js4));
+    IM3D_TRY(upload_jobs(ctx, "wl_s_j2", js2));
+    IM3D_TRY(upload_jobs(ctx, "wl_k_rhs", jr));
+    if constexpr (sizeof(T) == 4) IM3D_TRY(upload_jobs(ctx, "wl_fit", jfm));
+    else IM3D_TRY(upload_jobs(ctx, "wl_fit", jfw));
+    for (int c = 0; c < 2; ++c) {
+        if (neu) IM3D_TRY(upload_jobs(ctx, c ? "wl_rb1" : "wl_rb0", jrn[c]));
+        else IM3D_TRY(upload_jobs(ctx, c ? "wl_rb1" : "wl_rb0", jrd[c]));
+    }
+    IM3D_TRY(upload_jobs(ctx, "wl_residual", jres));
+    IM3D_TRY(upload_jobs(ctx, "wl_clamp_v", jclv));
+    IM3D_TRY(upload_jobs(ctx, "wl_clamp_s", jcls));
+    IM3D_TRY(upload_jobs(ctx, "wl_bregman_v", jbrv));
+    IM3D_TRY(upload_jobs(ctx, "wl_bregman_s", jbrs));
+    IM3D_TRY(upload_jobs(ctx, "wl_div_v", jdvv));
+    IM3D_TRY(upload_jobs(ctx, "wl_div_s", jdvs));
+    FinalizeJob *fin_res_d = nullptr, *fin_cl_d = nullptr;
+    IM3D_TRY(tbuf<FinalizeJob>(ctx, "wl_fin_res", nv, &fin_res_d));
+    IM3D_TRY(tbuf<FinalizeJob>(ctx, "wl_fin_clamp", nv, &fin_cl_d));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(fin_res_d, fin_res.data(), nv * sizeof(FinalizeJob), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    IM3D_CUDA(ctx, cudaMemcpyAsync(fin_cl_d, fin_cl.data(), nv * sizeof(FinalizeJob), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+
+    std::vector<WlCount> C(nv);
+    std::vector<double> tol(nv), sched_rate(nv);
+    std::vector<int> sched_first(nv), init_vars(nv);
+    for (int q = 0; q < nv; ++q) {
+        tol[q] = V[q].tollerance;
+        sched_first[q] = V[q].sched_first;
+        sched_rate[q] = V[q].sched_rate;
+        init_vars[q] = V[q].init_variables;
+    }
+    auto read_ctrls = [&]() -> int {
+        IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->wl_ctrl_h, ctrl, nv * sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+        return sync(ctx);
+    };
+    auto split = [&](const std::vector<int>& sel, std::vector<int>& a, std::vector<int>& b) {
+        a.clear();
+        b.clear();
+        for (int q : sel) (vecrow[q] ? a : b).push_back(q);
+    };
+    const size_t smem_k4 = k_win_smem<T, 4, S>(), smem_k2 = k_win_smem<T, 2, S>();
+    const size_t smem_s4 = s_win_smem<T, 4, S>(), smem_s2 = s_win_smem<T, 2, S>();
+    const dim3 blk_k(kKwT, kKwR), blk_s(TW, TY);
+    std::vector<int> act, solving, due, flags, sv, ss;
+    // a volume whose loop would not start (maxiter < 1) returns its initial level set
+    for (int q = 0; q < nv; ++q)
+        if (!(tol[q] > p->tol) || p->maxiter < 1) {
+            C[q].done = true;
+            IM3D_CUDA(ctx, cudaMemcpyAsync(vols[ids[q]].phi_out, V[q].phi, V[q].n * sizeof(T), cudaMemcpyDefault,
+                                           ctx->stream));
+        }
+    IM3D_TRY(sync(ctx));
+    for (int q = 0; q < nv; ++q)
+        if (C[q].done && latency_ms)
+            latency_ms[ids[q]] =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    for (int t = 1;; ++t) {
+        act.clear();
+        for (int q = 0; q < nv; ++q)
+            if (!C[q].done) act.push_back(q);
+        if (act.empty()) break;
+        // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
+        IM3D_TRY((wl_launch<KHeav, kKwT * kKwR, 3>(ctx, jk, act, nullptr, blk_k, smem_k4, "conv_k_heaviside")));
+        IM3D_TRY((wl_launch<SJ4, TW * TY, 2>(ctx, js4, act, nullptr, blk_s, smem_s4, "conv_s_j4")));
+        if constexpr (sizeof(T) == 4)
+            IM3D_TRY((wl_launch<FitM, 32 * kMarchJB, MarchMinB<S>::v>(ctx, jfm, act, nullptr, dim3(32, kMarchJB), 0,
+                                                                       "conv_i_fit")));
+        else
+            IM3D_TRY((wl_launch<FitW, TW * TY, 1>(ctx, jfw, act, nullptr, blk_s, fit_win_smem<T, S>(), "conv_i_fit")));
+        IM3D_TRY((wl_launch<SJ2, TW * TY, 3>(ctx, js2, act, nullptr, blk_s, smem_s2, "conv_s_j2")));
+        IM3D_TRY((wl_launch<KRhs, kKwT * kKwR, 3>(ctx, jr, act, nullptr, blk_k, smem_k2, "conv_k_rhs")));
+
+        // the Poisson step: rb_solve for every volume, the half-sweeps of all unconverged
+        // volumes in one launch, a residual check for each volume when its schedule
+        // (next_check) asks for one
+        const int maxs = std::max(p->gs_max_sweeps, 1);
+        const int every = std::max(p->gs_check_every, 0);
+        solving = act;
+        for (int q : act) {
+            WlCount& c = C[q];
+            c.s = 0;
+            c.s_prev = 0;
+            c.r_prev = -1;
+            c.rate_used = 0;
+            c.beff2 = -1;
+            c.rel = -1;
+            c.conv = false;
+            c.next = every > 0 ? every : (sched_first[q] > 0 ? sched_first[q] : 4);
+        }
+        const int pfs = prof_begin(ctx, "poisson_solve");
+        while (!solving.empty()) {
+            int k = maxs;
+            for (int q : solving) k = std::min(k, std::min(C[q].next, maxs) - C[q].s);
+            k = std::max(k, 1);
+            for (int i = 0; i < k; ++i)
+                for (int c = 0; c < 2; ++c) {
+                    if (neu)
+                        IM3D_TRY((wl_launch<RbN, 128, 1>(ctx, jrn[c], solving, nullptr, kBlkVec, 0, "rb_half", true)));
+                    else
+                        IM3D_TRY((wl_launch<RbD, 128, RB_MINB>(ctx, jrd[c], solving, nullptr, kBlkVec, 0, "rb_half",
+                                                               true)));
+                }
+            due.clear();
+            flags.clear();
+            for (int q : solving) {
+                C[q].s += k;
+                if (C[q].s >= C[q].next || C[q].s == maxs) {
+                    due.push_back(q);
+                    flags.push_back(C[q].beff2 < 0 ? 1 : 0);
+                }
+            }
+            IM3D_TRY((wl_launch<Res, 256, 2>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
+            IM3D_TRY(wl_finalize(ctx, fin_res_d, due, flags.data(), 1, SUM_RES2));
+            IM3D_TRY(read_ctrls());
+            std::vector<int> still;
+            for (int q : solving) {
+                WlCount& c = C[q];
+                const bool checked = c.s >= c.next || c.s == maxs;
+                if (checked) {
+                    ++c.checks;
+                    const Ctrl& cb = ctx->wl_ctrl_h[q];
+                    if (c.beff2 < 0) c.beff2 = cb.sum[SUM_BEFF2];
+                    const double rr = cb.sum[SUM_RES2];
+                    const double r = c.beff2 > 0 ? std::sqrt(rr) / std::sqrt(c.beff2) : std::sqrt(rr);
+                    c.rel = r;
+                    if (r <= p->gs_rel_res_tol) {
+                        c.conv = true;
+                        continue;
+                    }
+                    if (c.s >= maxs) continue;  // not converged
+                    c.next = next_check(c.s, r, c.s_prev, c.r_prev, p->gs_rel_res_tol, every, sched_rate[q],
+                                        &c.rate_used);
+                    if (c.next > maxs) c.next = maxs;
+                    c.s_prev = c.s;
+                    c.r_prev = r;
+                }
+                still.push_back(q);
+            }
+            solving.swap(still);
+        }
+        prof_end(ctx, pfs);
+        for (int q : act) {
+            WlCount& c = C[q];
+            const double rate = c.rate_used > 0 ? c.rate_used : sched_rate[q];
+            sched_first[q] = c.conv ? c.s : 0;
+            sched_rate[q] = c.conv ? rate : 0;
+            if (!c.conv) c.not_conv++;
+            c.total_sweeps += c.s;
+            c.last_sweeps = c.s;
+            c.last_rel = c.rel;
+        }
+
+        // clamp and tolerance, then the Bregman update and div(d - b)
+        split(act, sv, ss);
+        IM3D_TRY((wl_launch<ClV, 256, 4>(ctx, jclv, sv, nullptr, kBlkVec, 0, "clamp_tol")));
+        IM3D_TRY((wl_launch<ClS, 256, 1>(ctx, jcls, ss, nullptr, kBlkVol, 0, "clamp_tol")));
+        IM3D_TRY(wl_finalize(ctx, fin_cl_d, act, nullptr, 2, SUM_DPHI2));
+        IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->wl_ctrl_h, ctrl, nv * sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+        IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+        std::vector<int> upd;
+        for (int q : act) {
+            if (init_vars[q]) {
+                IM3D_CUDA(ctx, cudaMemsetAsync(V[q].divdb, 0, V[q].n * sizeof(T), ctx->stream));
+                IM3D_CUDA(ctx, cudaMemsetAsync(V[q].b3, 0, 3 * V[q].n * sizeof(T), ctx->stream));
+                init_vars[q] = 0;
+            } else {
+                upd.push_back(q);
+            }
+        }
+        split(upd, sv, ss);
+        IM3D_TRY((wl_launch<BrV, 256, 2>(ctx, jbrv, sv, nullptr, kBlkVec, 0, "bregman")));
+        IM3D_TRY((wl_launch<BrS, 256, 1>(ctx, jbrs, ss, nullptr, kBlkVol, 0, "bregman")));
+        IM3D_TRY((wl_launch<DvV, 256, 3>(ctx, jdvv, sv, nullptr, kBlkVec, 0, "div")));
+        IM3D_TRY((wl_launch<DvS, 256, 1>(ctx, jdvs, ss, nullptr, kBlkVol, 0, "div")));
+        if (cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) IM3D_TRY(sync(ctx));
+        for (int q : act) {
+            const Ctrl& cb = ctx->wl_ctrl_h[q];
+            tol[q] = std::sqrt(V[q].hhh * cb.sum[SUM_DPHI2]) / std::sqrt(V[q].hhh * cb.sum[SUM_PHIOLD2]);
+            C[q].iterations = t;
+            if (!(tol[q] > p->tol) || t + 1 > p->maxiter) C[q].done = true;
+        }
+        // volumes that finished: their result goes out now (latency)
+        bool any = false;
+        for (int q : act) any = any || C[q].done;
+        if (any) {
+            for (int q : act) {
+                if (!C[q].done) continue;
+                const im3d_volume_desc& dsc = vols[ids[q]];
+                IM3D_CUDA(ctx, cudaMemcpyAsync(dsc.phi_out, V[q].phi, V[q].n * sizeof(T), cudaMemcpyDefault,
+                                               ctx->stream));
+            }
+            IM3D_TRY(sync(ctx));
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start)
+                                  .count();
+            for (int q : act)
+                if (C[q].done && latency_ms) latency_ms[ids[q]] = ms;
+        }
+    }
+    if (stats) {
+        for (int q = 0; q < nv; ++q) {
+            im3d_rsfe_stats& st = stats[ids[q]];
+            std::memset(&st, 0, sizeof(st));
+            st.iterations = C[q].iterations;
+            st.last_tol = tol[q];
+            st.total_sweeps = C[q].total_sweeps;
+            st.last_sweeps = C[q].last_sweeps;
+            st.last_rel_res = C[q].last_rel;
+            st.last_ls_err = -1;
+            st.not_converged = C[q].not_conv;
+            st.residual_checks = C[q].checks;
+        }
+    }
+    return IM3D_OK;
+}
+
+// Work-list batch: groups of up to kMaxListVols volumes, largest first.
+template <typename T>
+int rsfe_apply_worklist(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols, const im3d_rsfe_params* p,
+                        int nh, im3d_rsfe_stats* stats, double* latency_ms)
+{
+    std::vector<int> order(nvol);
+    for (int v = 0; v < nvol; ++v) order[v] = v;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (long long)vols[a].nx * vols[a].ny * vols[a].nz > (long long)vols[b].nx * vols[b].ny * vols[b].nz;
+    });
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int g0 = 0; g0 < nvol; g0 += kMaxListVols) {
+        const std::vector<int> ids(order.begin() + g0, order.begin() + std::min(nvol, g0 + kMaxListVols));
+        if (nh == 19) IM3D_TRY((worklist_group<T, 9>(ctx, ids, vols, p, stats, latency_ms, t0)));
+        else IM3D_TRY((worklist_group<T, 12>(ctx, ids, vols, p, stats, latency_ms, t0)));
+    }
+    return IM3D_OK;
+}
+
 // Batch of independent volumes: a queue ordered largest first, drained by `streams`
 // host workers, each owning a worker context (stream + buffers) of the same device.
 template <typename T>
@@ -1767,6 +2407,27 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
 {
     if (nvol < 0 || (nvol > 0 && !vols) || !p) return fail(ctx, IM3D_ERR_INVALID_ARG, "bad batch");
     if (nvol == 0) return IM3D_OK;
+    if (ctx->batch_mode != IM3D_BATCH_STREAMS) {
+        // the work list runs valid volumes only; otherwise the stream queue reports each
+        // bad volume and segments the others
+        int st = check_params(ctx, p);
+        for (int v = 0; v < nvol && st == IM3D_OK; ++v) {
+            if (!vols[v].myim || !vols[v].phi_out)
+                st = fail(ctx, IM3D_ERR_INVALID_ARG, "volume " + std::to_string(v) + ": myim and phi_out are required");
+            else
+                st = check_dims(ctx, vols[v].nx, vols[v].ny, vols[v].nz, vols[v].hx, vols[v].hy, vols[v].hz);
+        }
+        int nh = 0;
+        if (st == IM3D_OK && worklist_eligible<T>(p, nvol, vols, &nh))
+            return rsfe_apply_worklist<T>(ctx, nvol, vols, p, nh, stats, latency_ms);
+        if (ctx->batch_mode == IM3D_BATCH_WORKLIST) {
+            if (st != IM3D_OK) return st;
+            return fail(ctx, IM3D_ERR_UNSUPPORTED, "the work-list batch needs a residual solve with omega 1, "
+                                                   "19 or 25 Gaussian taps on every axis and no "
+                                                   "connected-component extraction");
+        }
+        ctx->err.clear();
+    }
     if (streams <= 0) streams = 4;
     if (streams > nvol) streams = nvol;
     if (streams > 32) streams = 32;
@@ -1898,6 +2559,9 @@ int im3d_ctx_destroy(im3d_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (im3d_ctx* w : ctx->workers) im3d_ctx_destroy(w);
+    for (im3d_ctx* v : ctx->vols) im3d_ctx_destroy(v);
+    ctx->vols.clear();
+    if (ctx->wl_ctrl_h) cudaFreeHost(ctx->wl_ctrl_h);
     ctx->workers.clear();
     cudaSetDevice(ctx->device);
     for (auto& kv : ctx->bufs)
@@ -1933,6 +2597,10 @@ int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value)
     case IM3D_OPT_DEVICE_MEMORY_LIMIT:
         ctx->mem_limit = (size_t)value;
         for (im3d_ctx* w : ctx->workers) w->mem_limit = (size_t)value;
+        return IM3D_OK;
+    case IM3D_OPT_BATCH_MODE:
+        if (value > IM3D_BATCH_WORKLIST) return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown batch mode");
+        ctx->batch_mode = (int)value;
         return IM3D_OK;
     default:
         return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown option " + std::to_string(option));

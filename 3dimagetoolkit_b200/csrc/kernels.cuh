@@ -482,8 +482,7 @@ struct PairedFields {
 // row; tile RKR rows x 4*TKT k. The halo is rounded up to SP = 4*ceil(S/4) so that
 // every thread's window starts 16-byte aligned and is read with vector loads.
 template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
-__global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims d,
-                                                            const T* __restrict__ taps)
+__device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3 gridDim, Ld ld, St st, Dims d, const T* __restrict__ taps)
 {
     constexpr int R = 4;
     constexpr int TK = TKT * R;
@@ -598,11 +597,16 @@ __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims
     st.put4(pre, i, j, kk, vo, min(R, d.nz - kk));
 }
 
+template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
+__global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims d, const T* __restrict__ taps)
+{
+    conv_k_win_body<T, N, S, TKT, RKR, Ld, St>(blockIdx, gridDim, ld, st, d, taps);
+}
+
 // Along j (AXIS 1) or i (AXIS 0). Block TW x TY; each thread R consecutive outputs
 // along the axis in one k column; tile TY*R along the axis x TW along k.
 template <typename T, int N, int AXIS, int S, int TW, int TY, int R, class Ld, class St>
-__global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d,
-                                                          const T* __restrict__ taps)
+__device__ __forceinline__ void conv_s_win_body(const uint3 blockIdx, const dim3 gridDim, Ld ld, St st, Dims d, const T* __restrict__ taps)
 {
     constexpr int TA = TY * R;
     constexpr int H = TA + 2 * S;
@@ -685,15 +689,17 @@ __global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d
     }
 }
 
+template <typename T, int N, int AXIS, int S, int TW, int TY, int R, class Ld, class St>
+__global__ void __launch_bounds__(TW* TY) conv_s_win_kernel(Ld ld, St st, Dims d, const T* __restrict__ taps)
+{
+    conv_s_win_body<T, N, AXIS, S, TW, TY, R, Ld, St>(blockIdx, gridDim, ld, st, d, taps);
+}
+
 // Fused i-axis stage with register windows (see conv_i_fit_kernel for the maths).
 // First pass: RA = ceil((TA+2S)/TY) rows per thread over the four fields; second
 // pass: RB = TA/TY rows per thread over the pair.
 template <typename T, int S, int TW, int TY, int TA>
-__global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>* __restrict__ in,
-                                                              Vec<T, 2>* __restrict__ out,
-                                                              T* f1_out, T* f2_out, Dims d,
-                                                              const T* __restrict__ taps, T l1,
-                                                              T l2)
+__device__ __forceinline__ void conv_i_fit_win_body(const uint3 blockIdx, const dim3 gridDim, const Vec<T, 4>* __restrict__ in, Vec<T, 2>* __restrict__ out, T* f1_out, T* f2_out, Dims d, const T* __restrict__ taps, T l1, T l2)
 {
     constexpr int RA = (TA + 2 * S + TY - 1) / TY;
     constexpr int RB = TA / TY;
@@ -784,6 +790,12 @@ __global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>*
     }
 }
 
+template <typename T, int S, int TW, int TY, int TA>
+__global__ void __launch_bounds__(TW* TY) conv_i_fit_win_kernel(const Vec<T, 4>* __restrict__ in, Vec<T, 2>* __restrict__ out, T* f1_out, T* f2_out, Dims d, const T* __restrict__ taps, T l1, T l2)
+{
+    conv_i_fit_win_body<T, S, TW, TY, TA>(blockIdx, gridDim, in, out, f1_out, f2_out, d, taps, l1, l2);
+}
+
 // One step of a running convolution along a march axis, on float pairs with the
 // packed f32x2 pipes. acc[u] holds the partial sum of row p - S + u, where p is the
 // plane being added: acc[u] <- acc[u+1] + w[u] x for u = 0 .. 2S-1 (w symmetric,
@@ -846,10 +858,7 @@ struct TapPairs {
 // row adds its 2S+1 products in plane order, where the tiled kernels add symmetric
 // pairs first; f1 and f2 use the fast division (within 2 ulp).
 template <int S, int JB, int D, int U, int MINB>
-__global__ void __launch_bounds__(32 * JB, MINB)
-    conv_i_fit_march_kernel(const float4* __restrict__ in, float2* __restrict__ out,
-                            float* f1_out, float* f2_out, Dims d, const TapPairs<S> tp,
-                            float l1, float l2, int chunk)
+__device__ __forceinline__ void conv_i_fit_march_body(const uint3 blockIdx, const dim3 gridDim, const float4* __restrict__ in, float2* __restrict__ out, float* f1_out, float* f2_out, Dims d, const TapPairs<S> tp, float l1, float l2, int chunk)
 {
     constexpr int L = 2 * S + 1;
     static_assert((D & (D - 1)) == 0 && D >= 2 * U && D <= 16, "ring: a power of two, >= 2U");
@@ -920,6 +929,12 @@ __global__ void __launch_bounds__(32 * JB, MINB)
         for (int q = 0; q < U; ++q) issue(n0 + D - U + q);
     }
     cp_async_wait<0>();
+}
+
+template <int S, int JB, int D, int U, int MINB>
+__global__ void __launch_bounds__(32 * JB, MINB) conv_i_fit_march_kernel(const float4* __restrict__ in, float2* __restrict__ out, float* f1_out, float* f2_out, Dims d, const TapPairs<S> tp, float l1, float l2, int chunk)
+{
+    conv_i_fit_march_body<S, JB, D, U, MINB>(blockIdx, gridDim, in, out, f1_out, f2_out, d, tp, l1, l2, chunk);
 }
 
 // Fused i-axis stage: K_i applied to the four stage-1 fields (H u0, H, Hb u0, Hb)
@@ -1050,8 +1065,7 @@ __device__ __forceinline__ T div_point(const T* f0, const T* f1, const T* f2, co
 }
 
 template <typename T>
-__global__ void div_kernel(const T* __restrict__ v, T* __restrict__ out, Dims d, double hx,
-                           double hy, double hz)
+__device__ __forceinline__ void div_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ v, T* __restrict__ out, Dims d, double hx, double hy, double hz)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1059,6 +1073,12 @@ __global__ void div_kernel(const T* __restrict__ v, T* __restrict__ out, Dims d,
     if (k >= d.nz || j >= d.ny) return;
     const long long n = d.n();
     out[d.idx(i, j, k)] = div_point(v, v + n, v + 2 * n, d, i, j, k, hx, hy, hz);
+}
+
+template <typename T>
+__global__ void div_kernel(const T* __restrict__ v, T* __restrict__ out, Dims d, double hx, double hy, double hz)
+{
+    div_body<T>(blockIdx, gridDim, v, out, d, hx, hy, hz);
 }
 
 // Edge detector, GRAD branch (rsfe_splitbregman_imp.hxx:220-232, 308-313):
@@ -1237,11 +1257,7 @@ __device__ __forceinline__ double gs_residual_fp64(const GsCoef<T>& c, const Dim
 // half-sweep following one in the other direction starts on the planes that are still
 // in L2.
 template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
-__global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ U,
-                                                                const T* __restrict__ B, Dims d,
-                                                                GsCoef<T> c, int color,
-                                                                int use_self, T omega,
-                                                                int reverse = 0)
+__device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim3 gridDim, T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, int color, int use_self, T omega, int reverse)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -1365,13 +1381,16 @@ __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ 
     }
 }
 
+template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, int color, int use_self, T omega, int reverse = 0)
+{
+    rb_half_vec_body<T, NI, SELF, NEU, MINB>(blockIdx, gridDim, U, B, d, c, color, use_self, omega, reverse);
+}
+
 // Vectorised FP64 residual, same walk as rb_half_vec_kernel; blockIdx.z covers
 // (plane block, colour).
 template <typename T, int NI>
-__global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restrict__ U,
-                                                              const T* __restrict__ B, Dims d,
-                                                              GsCoef<T> c, double* part,
-                                                              int want_beff)
+__device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -1392,7 +1411,10 @@ __global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restric
         const bool jint = j >= 1 && j <= d.ny - 2;
         const int lo = c.neu ? 0 : 1;
         const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
-        VV o[NI + 2];
+        // every load of the NI planes is issued before the arithmetic (memory-level
+        // parallelism: the kernel waits on memory, not on its FP64 work)
+        VV o[NI + 2], bvv[NI], uvv[NI], ymv[NI], ypv[NI];
+        T exv[NI];
 #pragma unroll
         for (int t = 0; t < NI + 2; ++t) {
             const int i = i0 - 1 + t;
@@ -1402,18 +1424,33 @@ __global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restric
 #pragma unroll
         for (int t = 0; t < NI; ++t) {
             const int i = i0 + t;
-            if (i >= d.nx) break;
             const long long q = q0 + (long long)t * plane;
             const int par = (i + j + color) & 1;
-            const bool rowint = jint && i >= 1 && i <= d.nx - 2;
-            const VV bv = *reinterpret_cast<const VV*>(bb + q);
-            const VV uv = *reinterpret_cast<const VV*>(own + q);
-            if (rowint) {
-                const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
-                const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
-                const long long qe = par ? q + W : q - 1;
+            bvv[t] = uvv[t] = ymv[t] = ypv[t] = VV{};
+            exv[t] = T(0);
+            if (i < d.nx) {
+                bvv[t] = *reinterpret_cast<const VV*>(bb + q);
+                uvv[t] = *reinterpret_cast<const VV*>(own + q);
+            }
+            if (jint && i >= 1 && i <= d.nx - 2) {
+                ymv[t] = *reinterpret_cast<const VV*>(oth + q - hz);
+                ypv[t] = *reinterpret_cast<const VV*>(oth + q + hz);
                 const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
-                const double extra = e_ok ? (double)oth[qe] : 0.0;
+                if (e_ok) exv[t] = oth[par ? q + W : q - 1];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            const int i = i0 + t;
+            if (i >= d.nx) break;
+            const int par = (i + j + color) & 1;
+            const bool rowint = jint && i >= 1 && i <= d.nx - 2;
+            const VV bv = bvv[t];
+            const VV uv = uvv[t];
+            if (rowint) {
+                const VV ym = ymv[t];
+                const VV yp = ypv[t];
+                const double extra = (double)exv[t];
 #pragma unroll
                 for (int cc = 0; cc < W; ++cc) {
                     const int k = 2 * (m0 + cc) + par;
@@ -1446,8 +1483,14 @@ __global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restric
             }
         }
     }
-    if (want_beff) block_sum2_store(acc, accb, part);
-    else block_sum_store(acc, part);
+    if (want_beff) block_sum2_store(acc, accb, part, block_linear_id(blockIdx, gridDim), grid_blocks(gridDim));
+    else block_sum_store(acc, part, block_linear_id(blockIdx, gridDim));
+}
+
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
+{
+    rb_residual_vec_body<T, NI>(blockIdx, gridDim, U, B, d, c, part, want_beff);
 }
 
 
@@ -1455,9 +1498,7 @@ __global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restric
 // phi holds phiold on entry and the clamped solve result on exit (natural layout);
 // u is the solve result (packed or natural); u_out, when given, receives it unclamped.
 template <typename T, bool PACKED, int NI>
-__global__ void __launch_bounds__(256) clamp_tol_kernel(const T* __restrict__ u, T* phi,
-                                                        T* __restrict__ u_out, Dims d, T a0, T b0,
-                                                        double* part)
+__device__ __forceinline__ void clamp_tol_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ u, T* phi, T* __restrict__ u_out, Dims d, T a0, T b0, double* part)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1483,7 +1524,13 @@ __global__ void __launch_bounds__(256) clamp_tol_kernel(const T* __restrict__ u,
             s_o += (double)old * (double)old;
         }
     }
-    block_sum2_store(s_d, s_o, part);
+    block_sum2_store(s_d, s_o, part, block_linear_id(blockIdx, gridDim), grid_blocks(gridDim));
+}
+
+template <typename T, bool PACKED, int NI>
+__global__ void __launch_bounds__(256) clamp_tol_kernel(const T* __restrict__ u, T* phi, T* __restrict__ u_out, Dims d, T a0, T b0, double* part)
+{
+    clamp_tol_body<T, PACKED, NI>(blockIdx, gridDim, u, phi, u_out, d, a0, b0, part);
 }
 
 // The Split-Bregman update on the clamped phi (rsfe_splitbregman_imp.hxx:1868-1906),
@@ -1491,10 +1538,7 @@ __global__ void __launch_bounds__(256) clamp_tol_kernel(const T* __restrict__ u,
 // Thread per (k, j) column marching over NI planes with phi(i-1), phi(i), phi(i+1)
 // in registers; j and k neighbours come through L1.
 template <typename T, int NI>
-__global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
-                                                      T* __restrict__ b3, T* __restrict__ dmb,
-                                                      const T* __restrict__ g, Dims d, double hx,
-                                                      double hy, double hz)
+__device__ __forceinline__ void bregman_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ phi, T* __restrict__ b3, T* __restrict__ dmb, const T* __restrict__ g, Dims d, double hx, double hy, double hz)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1537,6 +1581,12 @@ __global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
     }
 }
 
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi, T* __restrict__ b3, T* __restrict__ dmb, const T* __restrict__ g, Dims d, double hx, double hy, double hz)
+{
+    bregman_body<T, NI>(blockIdx, gridDim, phi, b3, dmb, g, d, hx, hy, hz);
+}
+
 // ---- vectorised natural-layout kernels (nz a multiple of W = 16/sizeof(T)) ----
 // Thread per group of W consecutive k of row j, marching over NI planes of i.
 
@@ -1544,9 +1594,7 @@ __global__ void __launch_bounds__(256) bregman_kernel(const T* __restrict__ phi,
 // natural k = kb .. kb+W-1 (kb even) the even k sit in the colour array of (i+j)&1 and
 // the odd k in the other, both at m = kb/2 .. kb/2 + W/2 - 1.
 template <typename T, bool PACKED, int NI>
-__global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict__ u, T* phi,
-                                                            T* __restrict__ u_out, Dims d, T a0,
-                                                            T b0, double* part)
+__device__ __forceinline__ void clamp_tol_vec_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ u, T* phi, T* __restrict__ u_out, Dims d, T a0, T b0, double* part)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -1595,16 +1643,19 @@ __global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict_
             *reinterpret_cast<VV*>(phi + p) = nv;
         }
     }
-    block_sum2_store(s_d, s_o, part);
+    block_sum2_store(s_d, s_o, part, block_linear_id(blockIdx, gridDim), grid_blocks(gridDim));
+}
+
+template <typename T, bool PACKED, int NI>
+__global__ void __launch_bounds__(256) clamp_tol_vec_kernel(const T* __restrict__ u, T* phi, T* __restrict__ u_out, Dims d, T a0, T b0, double* part)
+{
+    clamp_tol_vec_body<T, PACKED, NI>(blockIdx, gridDim, u, phi, u_out, d, a0, b0, part);
 }
 
 // Split-Bregman update (see bregman_kernel), vectorised along k; rows on an i or j face
 // of the volume take the scalar one-sided stencils.
 template <typename T, int NI>
-__global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ phi,
-                                                          T* __restrict__ b3, T* __restrict__ dmb,
-                                                          const T* __restrict__ g3, Dims d,
-                                                          double hx, double hy, double hz)
+__device__ __forceinline__ void bregman_vec_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ phi, T* __restrict__ b3, T* __restrict__ dmb, const T* __restrict__ g3, Dims d, double hx, double hy, double hz)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -1715,11 +1766,16 @@ __global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ 
     }
 }
 
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) bregman_vec_kernel(const T* __restrict__ phi, T* __restrict__ b3, T* __restrict__ dmb, const T* __restrict__ g3, Dims d, double hx, double hy, double hz)
+{
+    bregman_vec_body<T, NI>(blockIdx, gridDim, phi, b3, dmb, g3, d, hx, hy, hz);
+}
+
 // im3d::div vectorised along k (see div_point); rows on an i or j face of the volume
 // take the scalar rule with the reference's quirks.
 template <typename T, int NI>
-__global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T* __restrict__ out,
-                                                      Dims d, double hx, double hy, double hz)
+__device__ __forceinline__ void div_vec_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ v, T* __restrict__ out, Dims d, double hx, double hy, double hz)
 {
     typedef V16<T> VT;
     typedef typename VT::type VV;
@@ -1790,6 +1846,12 @@ __global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T
     }
 }
 
+template <typename T, int NI>
+__global__ void __launch_bounds__(256) div_vec_kernel(const T* __restrict__ v, T* __restrict__ out, Dims d, double hx, double hy, double hz)
+{
+    div_vec_body<T, NI>(blockIdx, gridDim, v, out, d, hx, hy, hz);
+}
+
 // sum (a - b)^2 and sum b^2 over n elements (relative change of a sweep)
 template <typename T>
 __global__ void diff_sums_kernel(const T* __restrict__ a, const T* __restrict__ b, long long n,
@@ -1802,7 +1864,7 @@ __global__ void diff_sums_kernel(const T* __restrict__ a, const T* __restrict__ 
         sd += x * x;
         sb += (double)b[q] * (double)b[q];
     }
-    block_sum2_store(sd, sb, part);
+    block_sum2_store(sd, sb, part, block_linear_id(blockIdx, gridDim), grid_blocks(gridDim));
 }
 
 // natural -> packed copy of a volume (both colours), and back
@@ -1848,7 +1910,7 @@ __global__ void make_beff_kernel(const T* __restrict__ b, T* __restrict__ U, T* 
         Beff[pq] = e;
         if (!(dirichlet && face)) acc = (double)e * (double)e;
     }
-    if (part) block_sum_store(acc, part);
+    if (part) block_sum_store(acc, part, block_linear_id(blockIdx, gridDim));
 }
 
 

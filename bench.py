@@ -559,6 +559,8 @@ def run_batch(args):
         kw["maxiter"] = args.maxiter
     params = pkg.default_params(**kw)
     ctx = pkg.Context(local)
+    mode = {"auto": pkg.BATCH_AUTO, "streams": pkg.BATCH_STREAMS, "worklist": pkg.BATCH_WORKLIST}[args.batch_mode]
+    ctx.set_option(pkg.OPT_BATCH_MODE, mode)
     for _ in range(args.warmup):
         ctx.rsfe_apply_batched(vols, inits, params, streams=args.streams, outs=outs)
     torch.cuda.synchronize()
@@ -585,7 +587,8 @@ def run_batch(args):
             "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (48 seeded two-ellipsoid volumes)",
             "config": {"workload": "48 volumes 96..256 x 96..256 x 64..192, 100 outer iterations",
-                       "streams": args.streams, "volumes_per_rank": len(mine)},
+                       "batch_mode": args.batch_mode, "streams": args.streams,
+                       "volumes_per_rank": len(mine)},
             "latency_ms": {"p50": float(np.percentile(lats, 50)), "p95": float(np.percentile(lats, 95))},
             "gpu_launches": launches,
             "timing": "host wall clock around the batched calls (each call returns after all "
@@ -774,6 +777,8 @@ def main():
                     help="c2: one 256^3 volume per step (default); c3: 512x512x320 CT-like "
                          "volume, sigma 4, 200 iterations; batch: 48 uneven volumes")
     ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent streams")
+    ap.add_argument("--batch-mode", default="auto", choices=["auto", "streams", "worklist"],
+                    help="batch workload: work list (auto picks it for this workload) or stream queue")
     ap.add_argument("--size", type=int, default=0,
                     help="profiling only: cube side of a smaller/larger case (default 256)")
     ap.add_argument("--maxiter", type=int, default=0,

@@ -144,9 +144,18 @@ int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
  *                                that would need more returns IM3D_ERR_OOM before it
  *                                allocates (0, the default, = no limit). For callers that
  *                                share the GPU under a memory budget.
+ *  IM3D_OPT_BATCH_MODE           how im3d_rsfe_apply_batched_* runs its volumes:
+ *                                IM3D_BATCH_AUTO (default) = the work list whenever the
+ *                                parameters allow it, else the stream queue;
+ *                                IM3D_BATCH_STREAMS = the stream queue; IM3D_BATCH_WORKLIST
+ *                                = the work list, IM3D_ERR_UNSUPPORTED where it cannot run.
  * Returns IM3D_ERR_INVALID_ARG for an unknown option or a negative value. */
 #define IM3D_OPT_FIT_CHUNKS 1
 #define IM3D_OPT_DEVICE_MEMORY_LIMIT 2
+#define IM3D_OPT_BATCH_MODE 3
+#define IM3D_BATCH_AUTO 0
+#define IM3D_BATCH_STREAMS 1
+#define IM3D_BATCH_WORKLIST 2
 int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value);
 /* Per-stage device timing: with profiling on, each launch of the loop's kernels is
  * bracketed by CUDA events on the launching stream. im3d_ctx_profile() synchronises,
@@ -386,12 +395,22 @@ typedef struct im3d_volume_desc {
     double hx, hy, hz;
 } im3d_volume_desc;
 
-/* Segments nvol volumes with the same parameters. Volumes are taken largest first from
- * a shared queue by `streams` workers (0 = 4), each running whole segmentations on
- * its own CUDA stream with its own device buffers, so small volumes overlap on the
- * GPU. stats and latency_ms (either may be NULL) receive nvol entries: the statistics
- * of each volume and the time from the start of the call to that volume's result.
- * Returns the first non-OK status (the other volumes still run). */
+/* Segments nvol volumes with the same parameters, in one of two ways
+ * (IM3D_OPT_BATCH_MODE):
+ *  - the work list: groups of up to 64 volumes, largest first, advance their outer
+ *    iterations together, and each stage of the loop is ONE launch over the blocks of
+ *    every volume of the group that still runs it (each Poisson half-sweep over the
+ *    volumes whose solve has not converged, each residual check over those due for
+ *    one). Runs when the Poisson step is solved to a residual (gs_rel_res_tol > 0,
+ *    omega 1), the Gaussian has 19 or 25 taps on every axis of every volume and no
+ *    connected-component extraction is asked for; `streams` is then unused.
+ *  - the stream queue: volumes are taken largest first from a shared queue by
+ *    `streams` workers (0 = 4), each running whole segmentations on its own CUDA
+ *    stream with its own device buffers, so small volumes overlap on the GPU.
+ * Both give every volume the result of its own im3d_rsfe_apply_* call, bit for bit.
+ * stats and latency_ms (either may be NULL) receive nvol entries: the statistics of
+ * each volume and the time from the start of the call to that volume's result.
+ * Returns the first non-OK status. */
 int im3d_rsfe_apply_batched_f32(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
                                 const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats,
                                 double* latency_ms);

@@ -37,3 +37,23 @@ def test_no_device_is_reported_not_faked(pkg):
     with pytest.raises(pkg.Im3dError) as e:
         pkg.Context(0)
     assert e.value.status == 6
+
+
+def test_python_constants_match_the_header(pkg):
+    """Every IM3D_ status, option, batch-mode, boundary, sweep and warm-start constant of
+    include/im3d_b200.h has the same value in the Python binding."""
+    import os
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "im3d_b200.h")).read()
+    defs = dict(re.findall(r"#define IM3D_([A-Z0-9_]+) \(?(-?\d+)\)?", hdr))
+    prefixes = ("ERR_", "OPT_", "BATCH_", "BC_", "SWEEP_", "WS_")
+    checked = 0
+    for name, value in defs.items():
+        if name.startswith(prefixes) and hasattr(pkg._abi, name):
+            assert getattr(pkg._abi, name) == int(value), name
+            checked += 1
+    for must in ("OPT_BATCH_MODE", "BATCH_AUTO", "BATCH_STREAMS", "BATCH_WORKLIST", "ERR_NONFINITE"):
+        assert must in defs and hasattr(pkg._abi, must), must
+    assert checked >= 20
