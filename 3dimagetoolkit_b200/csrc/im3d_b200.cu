@@ -56,6 +56,8 @@ struct im3d_ctx {
     struct Pending {
         std::string name;
         cudaEvent_t a, b;
+        bool closed;  // b recorded (prof_end)
+        bool done;    // folded into the totals
     };
     std::vector<Pending> pending;
     struct Acc {
@@ -144,7 +146,7 @@ int prof_begin(im3d_ctx* ctx, const char* name)
 {
     if (!ctx->prof) return -1;
     if (ctx->prof == 2 && std::strcmp(name, "poisson_solve") != 0) return -1;
-    im3d_ctx::Pending pd{name, prof_event(ctx), prof_event(ctx)};
+    im3d_ctx::Pending pd{name, prof_event(ctx), prof_event(ctx), false, false};
     cudaEventRecord(pd.a, ctx->stream);
     ctx->pending.push_back(pd);
     return (int)ctx->pending.size() - 1;
@@ -152,13 +154,24 @@ int prof_begin(im3d_ctx* ctx, const char* name)
 
 void prof_end(im3d_ctx* ctx, int slot)
 {
-    if (slot >= 0) cudaEventRecord(ctx->pending[slot].b, ctx->stream);
+    if (slot < 0) return;
+    cudaEventRecord(ctx->pending[slot].b, ctx->stream);
+    ctx->pending[slot].closed = true;
 }
 
-// After a stream synchronisation: fold the pending event pairs into the totals.
+// After a stream synchronisation: fold the closed event pairs into the totals. A
+// stage that encloses synchronisations (the whole Poisson solve) stays pending until
+// it is closed; the slots keep their indices until every pair is folded.
 void prof_resolve(im3d_ctx* ctx)
 {
+    bool all = true;
     for (auto& pd : ctx->pending) {
+        if (pd.done) continue;
+        if (!pd.closed) {
+            all = false;
+            continue;
+        }
+        pd.done = true;
         float ms = 0;
         if (cudaEventElapsedTime(&ms, pd.a, pd.b) != cudaSuccess) {
             cudaGetLastError();
@@ -181,7 +194,7 @@ void prof_resolve(im3d_ctx* ctx)
         ctx->ev_pool.push_back(pd.a);
         ctx->ev_pool.push_back(pd.b);
     }
-    ctx->pending.clear();
+    if (all) ctx->pending.clear();
 }
 
 // Device buffer of at least `bytes` under `name`, reused across calls.
@@ -620,6 +633,7 @@ GsCoef<T> make_coef(double hx, double hy, double hz, double dt, double bc, int n
         double cx = (m & 1) ? 2. : 1., cy = (m & 2) ? 2. : 1., cz = (m & 4) ? 2. : 1.;
         double ht = 1. / dt + cx / (hx * hx) + cy / (hy * hy) + cz / (hz * hz);
         c.htilde[m] = (T)(1. / ht);
+        c.htilde_lo[m] = sizeof(T) == 4 ? (T)(1. / ht - (double)c.htilde[m]) : T(0);
     }
     // oblique normals of NeuGaussSeidel (poisson_imp.hxx:155-159): 1, 1/sqrt2, 1/sqrt3
     const T tb = (T)bc;

@@ -449,34 +449,12 @@ __device__ __forceinline__ void window_conv(const T (&x)[R + 2 * S], const T (&w
     }
 }
 
-// The same on two fields at once with the packed f32x2 instructions of sm_100 (the
-// operations of window_conv, lane by lane: identical results, half the instructions).
-template <int S, int R>
-__device__ __forceinline__ void window_conv2(const float2 (&x)[R + 2 * S], const float2 (&w)[S + 1],
-                                             float2 (&out)[R])
-{
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        float2 acc = __fmul2_rn(w[S], x[r + S]);
-#pragma unroll
-        for (int t = 0; t < S; ++t) acc = __ffma2_rn(w[t], __fadd2_rn(x[r + t], x[r + 2 * S - t]), acc);
-        out[r] = acc;
-    }
-}
-
 template <typename T, int S>
 __device__ __forceinline__ void load_taps(const T* __restrict__ taps, T (&w)[S + 1])
 {
 #pragma unroll
     for (int t = 0; t <= S; ++t) w[t] = __ldg(taps + t);
 }
-
-// FP32 passes with an even number of fields keep them in shared memory as float pairs
-// and convolve a pair per packed instruction
-template <typename T, int N>
-struct PairedFields {
-    static constexpr bool value = sizeof(T) == 4 && N % 2 == 0;
-};
 
 // Along k (contiguous). Block TKT x RKR threads; each thread 4 consecutive k of one
 // row; tile RKR rows x 4*TKT k. The halo is rounded up to SP = 4*ceil(S/4) so that
@@ -519,15 +497,8 @@ __device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.x + u * TKT;
             if (s < W) {
-                if constexpr (PairedFields<T, N>::value) {
-                    float2* sm2 = reinterpret_cast<float2*>(sm);  // [N/2][RKR][W] pairs
 #pragma unroll
-                    for (int q = 0; q < N / 2; ++q)
-                        sm2[(q * RKR + threadIdx.y) * W + s] = make_float2(v[u].v[2 * q], v[u].v[2 * q + 1]);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < N; ++q) sm[(q * RKR + threadIdx.y) * W + s] = v[u].v[q];
-                }
+                for (int q = 0; q < N; ++q) sm[(q * RKR + threadIdx.y) * W + s] = v[u].v[q];
             }
         }
     }
@@ -536,34 +507,7 @@ __device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3
     __syncthreads();
     const bool act = live && kk < d.nz;
     T res[N][R];
-    if constexpr (PairedFields<T, N>::value) {
-        if (act) {
-            float2 w2[S + 1];
-#pragma unroll
-            for (int t = 0; t <= S; ++t) w2[t] = make_float2(w[t], w[t]);
-#pragma unroll
-            for (int q = 0; q < N / 2; ++q) {
-                const float2* base = reinterpret_cast<const float2*>(sm) + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
-                float2 xa[XW];
-#pragma unroll
-                for (int t = 0; t < XW; t += 2) {
-                    const float4 v4 = *reinterpret_cast<const float4*>(base + t);
-                    xa[t] = make_float2(v4.x, v4.y);
-                    xa[t + 1] = make_float2(v4.z, v4.w);
-                }
-                float2 x[R + 2 * S];
-#pragma unroll
-                for (int t = 0; t < R + 2 * S; ++t) x[t] = xa[t + SP - S];
-                float2 o[R];
-                window_conv2<S, R>(x, w2, o);
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    res[2 * q][r] = o[r].x;
-                    res[2 * q + 1][r] = o[r].y;
-                }
-            }
-        }
-    } else if (act) {
+    if (act) {
 #pragma unroll
         for (int q = 0; q < N; ++q) {
             const T* base = sm + (q * RKR + threadIdx.y) * W + threadIdx.x * R;
@@ -631,15 +575,8 @@ __device__ __forceinline__ void conv_s_win_body(const uint3 blockIdx, const dim3
         for (int u = 0; u < NL; ++u) {
             const int s = threadIdx.y + u * TY;
             if (s < H) {
-                if constexpr (PairedFields<T, N>::value) {
-                    float2* sm2 = reinterpret_cast<float2*>(sm);  // [N/2][H][TW] pairs
 #pragma unroll
-                    for (int q = 0; q < N / 2; ++q)
-                        sm2[(q * H + s) * TW + threadIdx.x] = make_float2(v[u].v[2 * q], v[u].v[2 * q + 1]);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < N; ++q) sm[(q * H + s) * TW + threadIdx.x] = v[u].v[q];
-                }
+                for (int q = 0; q < N; ++q) sm[(q * H + s) * TW + threadIdx.x] = v[u].v[q];
             }
         }
     }
@@ -649,25 +586,6 @@ __device__ __forceinline__ void conv_s_win_body(const uint3 blockIdx, const dim3
     if (!kin) return;
     const int r0 = threadIdx.y * R;
     Vec<T, N> out[R];
-    if constexpr (PairedFields<T, N>::value) {
-        float2 w2[S + 1];
-#pragma unroll
-        for (int t = 0; t <= S; ++t) w2[t] = make_float2(w[t], w[t]);
-        const float2* sm2 = reinterpret_cast<const float2*>(sm);
-#pragma unroll
-        for (int q = 0; q < N / 2; ++q) {
-            float2 x[R + 2 * S];
-#pragma unroll
-            for (int t = 0; t < R + 2 * S; ++t) x[t] = sm2[(q * H + r0 + t) * TW + threadIdx.x];
-            float2 o[R];
-            window_conv2<S, R>(x, w2, o);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                out[r].v[2 * q] = o[r].x;
-                out[r].v[2 * q + 1] = o[r].y;
-            }
-        }
-    } else {
 #pragma unroll
     for (int q = 0; q < N; ++q) {
         T x[R + 2 * S];
@@ -677,7 +595,6 @@ __device__ __forceinline__ void conv_s_win_body(const uint3 blockIdx, const dim3
         window_conv<T, S, R>(x, w, o);
 #pragma unroll
         for (int r = 0; r < R; ++r) out[r].v[q] = o[r];
-    }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -1115,6 +1032,12 @@ struct GsCoef {
     // reciprocal form (float)
     T ihx2, ihy2, ihz2, idt;
     T htilde[8];   // indexed by (cx inside) | (cy inside) << 1 | (cz inside) << 2
+    // FP32: the rounding of each reciprocal, htilde_lo = 1/ht - htilde. The update
+    // fma(acc, htilde, acc * htilde_lo) multiplies by 1/ht to within the final
+    // rounding; acc * htilde alone would scale every update by the same relative
+    // error (-2.6e-8 for 1/7), a bias of the operator that the outer iterations
+    // accumulate. Unused (zero) in FP64, which keeps the reference's form.
+    T htilde_lo[8];
     T bcn[4];      // bc scaled by the oblique normal for 1, 2, 3 boundary axes
     double bcnd[4];
     T bc;
@@ -1141,7 +1064,7 @@ __device__ __forceinline__ T gs_value(const GsCoef<T>& c, const Dims& d, int i, 
         } else {
             T acc = sx * c.ihx2 + sy * c.ihy2 + sz * c.ihz2 + b;
             if (use_self) acc += self * c.idt;
-            return acc * c.htilde[7];
+            return fma(acc, c.htilde[7], acc * c.htilde_lo[7]);
         }
     }
     const int cx = i == 0 ? 0 : (i == d.nx - 1 ? 2 : 1);
@@ -1171,7 +1094,8 @@ __device__ __forceinline__ T gs_value(const GsCoef<T>& c, const Dims& d, int i, 
                       : (cz == 0 ? r(0, 0, 1) - bcn * hz : r(0, 0, -1) + bcn * hz)) * c.ihz2;
         T acc = tx + ty + tz + b;
         if (use_self) acc += self * c.idt;
-        return acc * c.htilde[(cx == 1) | ((cy == 1) << 1) | ((cz == 1) << 2)];
+        const int m = (cx == 1) | ((cy == 1) << 1) | ((cz == 1) << 2);
+        return fma(acc, c.htilde[m], acc * c.htilde_lo[m]);
     }
 }
 
@@ -1349,7 +1273,7 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
                 } else {
                     T acc = fma(sx, c.ihx2, fma(sy, c.ihy2, fma(sz, c.ihz2, b)));
                     if (use_self) acc = fma(sf, c.idt, acc);
-                    v = acc * c.htilde[7];
+                    v = fma(acc, c.htilde[7], acc * c.htilde_lo[7]);
                 }
                 if (relax) v = sf + omega * (v - sf);
                 VT::set(outv, cc, v);

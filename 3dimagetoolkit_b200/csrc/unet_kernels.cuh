@@ -254,7 +254,7 @@ struct WgradArgs {
     int xcoff;       // first input channel in X's tensor
     int tap0, ntaps; // taps of this launch's blockIdx.x group: tap0 + blockIdx.x * ntaps ...
     int cout;        // output channels (rows of dZ used)
-    float* dw;       // FP32 gradient [cout][27][CIN], accumulated with atomics
+    float* dw;       // FP32 gradient [cout][CIN][27] (the parameter layout), accumulated with atomics
     int* err;
 };
 
@@ -362,9 +362,10 @@ __global__ void __launch_bounds__(128, 1) wgrad_tc_kernel(const __grid_constant_
                 float v[16];
                 tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ti * CIN + c0), v);
                 if (lane < 16 && co < a.cout) {
-                    float* d = a.dw + ((size_t)co * 27 + (t_first + ti)) * CIN + c0;
+                    // the parameter layout [cout][CIN][27]
+                    float* d = a.dw + ((size_t)co * CIN + c0) * 27 + (t_first + ti);
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) atomicAdd(d + u, v[u]);
+                    for (int u = 0; u < 16; ++u) atomicAdd(d + u * 27, v[u]);
                 }
             }
         }
