@@ -403,14 +403,20 @@ int set_smem(im3d_ctx* ctx, K kernel, size_t bytes)
     return IM3D_OK;
 }
 
-// Register-window k pass: blocks of RKR rows x TKT threads, 4 outputs per thread.
+// Register-window k pass: blocks of RKR rows x TKT threads, 4 RG outputs per thread.
 constexpr int kKwT = 32, kKwR = 8;
+template <typename T, int N> struct KWinRG { static constexpr int v = 1; };
 template <typename T, int N, int S>
-constexpr size_t k_win_smem() { return (size_t)N * kKwR * (kKwT * 4 + 2 * ((S + 3) & ~3)) * sizeof(T); }
+constexpr size_t k_win_smem()
+{
+    return (size_t)N * kKwR * (kKwT * 4 * KWinRG<T, N>::v + 2 * ((S + 3) & ~3)) * sizeof(T);
+}
+template <typename T, int N>
 dim3 k_win_grid(const Dims& d)
 {
+    constexpr int TK = kKwT * 4 * KWinRG<T, N>::v;
     const long long rows = (long long)d.nx * d.ny;
-    return dim3((unsigned)((rows + kKwR - 1) / kKwR), (d.nz + kKwT * 4 - 1) / (kKwT * 4));
+    return dim3((unsigned)((rows + kKwR - 1) / kKwR), (d.nz + TK - 1) / TK);
 }
 
 template <typename T, int N, int S, class Ld, class St>
@@ -418,9 +424,9 @@ int pass_k_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const cha
 {
     constexpr int TKT = kKwT, RKR = kKwR;
     const size_t smem = k_win_smem<T, N, S>();
-    auto kern = conv_k_win_kernel<T, N, S, TKT, RKR, Ld, St>;
+    auto kern = conv_k_win_kernel<T, N, S, TKT, RKR, Ld, St, KWinRG<T, N>::v>;
     IM3D_TRY(set_smem(ctx, kern, smem));
-    const dim3 grid = k_win_grid(d);
+    const dim3 grid = k_win_grid<T, N>(d);
     const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TKT, RKR), smem, ctx->stream>>>(ld, st, d, w);
     prof_end(ctx, pf);
@@ -2091,10 +2097,10 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
 
     // job tables: every stage's arguments and grid, per volume
     constexpr int R = SWinR<T>::v;
-    using KHeav = ConvKWinJob<T, 4, S, kKwT, kKwR, LdHeaviside<T>, StVec<T, 4>>;
+    using KHeav = ConvKWinJob<T, 4, S, kKwT, kKwR, LdHeaviside<T>, StVec<T, 4>, KWinRG<T, 4>::v>;
     using SJ4 = ConvSWinJob<T, 4, 1, S, TW, TY, R, LdVec<T, 4>, StVec<T, 4>>;
     using SJ2 = ConvSWinJob<T, 2, 1, S, TW, TY, R, LdVec<T, 2>, StVec<T, 2>>;
-    using KRhs = ConvKWinJob<T, 2, S, kKwT, kKwR, LdVec<T, 2>, StRhs<T>>;
+    using KRhs = ConvKWinJob<T, 2, S, kKwT, kKwR, LdVec<T, 2>, StRhs<T>, KWinRG<T, 2>::v>;
     using FitM = FitMarchJob<S, kMarchJB, kMarchD, kMarchU, MarchMinB<S>::v>;
     using FitW = FitWinJob<T, S, TW, TY, TileA<T>::v>;
     constexpr int RB_MINB = sizeof(T) == 4 ? 8 : 1;
@@ -2130,7 +2136,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         const Dims& d = v.d;
         const double hx = vols[ids[q]].hx, hy = vols[ids[q]].hy, hz = vols[ids[q]].hz;
         jk.h.push_back({KHeav{LdHeaviside<T>{v.phi, v.u0, d, v.center, v.inv_eps}, StVec<T, 4>{v.W1, d}, d,
-                              v.tp.w[2]}, k_win_grid(d)});
+                              v.tp.w[2]}, k_win_grid<T, 4>(d)});
         js4.h.push_back({SJ4{LdVec<T, 4>{v.W1, d}, StVec<T, 4>{v.W2, d}, d, v.tp.w[1]}, s_win_grid<T, 1>(d)});
         js2.h.push_back({SJ2{LdVec<T, 2>{v.P1, d}, StVec<T, 2>{v.P2, d}, d, v.tp.w[1]}, s_win_grid<T, 1>(d)});
         StRhs<T> st;
@@ -2146,7 +2152,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         st.bc = (T)v.chosen_bc;
         st.mode = 2;
         st.dirichlet = neu ? 0 : 1;
-        jr.h.push_back({KRhs{LdVec<T, 2>{v.P2, d}, st, d, v.tp.w[2]}, k_win_grid(d)});
+        jr.h.push_back({KRhs{LdVec<T, 2>{v.P2, d}, st, d, v.tp.w[2]}, k_win_grid<T, 2>(d)});
         if constexpr (sizeof(T) == 4) {
             dim3 g;
             const int chunk = march_chunk<S>(ctx->vols[q], d, &g);

@@ -456,13 +456,16 @@ __device__ __forceinline__ void load_taps(const T* __restrict__ taps, T (&w)[S +
     for (int t = 0; t <= S; ++t) w[t] = __ldg(taps + t);
 }
 
-// Along k (contiguous). Block TKT x RKR threads; each thread 4 consecutive k of one
-// row; tile RKR rows x 4*TKT k. The halo is rounded up to SP = 4*ceil(S/4) so that
-// every thread's window starts 16-byte aligned and is read with vector loads.
-template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
-__device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3 gridDim, Ld ld, St st, Dims d, const T* __restrict__ taps)
+// Along k (contiguous). Block TKT x RKR threads; each thread R = 4 RG consecutive k of
+// one row (RG groups of 4 for the storer); tile RKR rows x R*TKT k. The halo is rounded
+// up to SP = 4*ceil(S/4) so that every thread's window starts 16-byte aligned and is
+// read with vector loads. Larger RG reads fewer window values per output from shared
+// memory and recomputes fewer halo cells; every output is the same sum either way.
+template <typename T, int N, int S, int TKT, int RKR, class Ld, class St, int RG = 1>
+__device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3 gridDim, Ld ld, St st, Dims d,
+                                                const T* __restrict__ taps)
 {
-    constexpr int R = 4;
+    constexpr int R = 4 * RG;
     constexpr int TK = TKT * R;
     constexpr int SP = (S + 3) & ~3;
     constexpr int W = TK + 2 * SP;
@@ -475,7 +478,7 @@ __device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3
     const int j = live ? (int)(row % d.ny) : 0;
     const int k0 = blockIdx.y * TK;
     const int kk = k0 + threadIdx.x * R;  // this thread's first output cell (even)
-    typename St::Pre pre{};
+    typename St::Pre pre[RG]{};
     {
         constexpr int NL = (W + TKT - 1) / TKT;
         // all reads first, then the loader's arithmetic (the Heaviside for stage 1)
@@ -489,7 +492,9 @@ __device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3
             if (ok[u]) rw[u] = ld.raw(i, j, k);
         }
         // the storer's own reads (the forcing term's fields) go out with them
-        if (kk < d.nz && live) pre = st.pre(i, j, kk, min(R, d.nz - kk));
+#pragma unroll
+        for (int g = 0; g < RG; ++g)
+            if (kk + 4 * g < d.nz && live) pre[g] = st.pre(i, j, kk + 4 * g, min(4, d.nz - kk - 4 * g));
         Vec<T, N> v[NL];
 #pragma unroll
         for (int u = 0; u < NL; ++u) v[u] = ok[u] ? ld.cook(rw[u]) : vzero<T, N>();
@@ -532,19 +537,24 @@ __device__ __forceinline__ void conv_k_win_body(const uint3 blockIdx, const dim3
         }
     }
     if (!act) return;
-    Vec<T, N> vo[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
+    for (int g = 0; g < RG; ++g) {
+        const int kg = kk + 4 * g;
+        if (kg >= d.nz) break;
+        Vec<T, N> vo[4];
 #pragma unroll
-        for (int q = 0; q < N; ++q) vo[r].v[q] = res[q][r];
+        for (int r = 0; r < 4; ++r) {
+#pragma unroll
+            for (int q = 0; q < N; ++q) vo[r].v[q] = res[q][4 * g + r];
+        }
+        st.put4(pre[g], i, j, kg, vo, min(4, d.nz - kg));
     }
-    st.put4(pre, i, j, kk, vo, min(R, d.nz - kk));
 }
 
-template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
+template <typename T, int N, int S, int TKT, int RKR, class Ld, class St, int RG = 1>
 __global__ void __launch_bounds__(TKT* RKR) conv_k_win_kernel(Ld ld, St st, Dims d, const T* __restrict__ taps)
 {
-    conv_k_win_body<T, N, S, TKT, RKR, Ld, St>(blockIdx, gridDim, ld, st, d, taps);
+    conv_k_win_body<T, N, S, TKT, RKR, Ld, St, RG>(blockIdx, gridDim, ld, st, d, taps);
 }
 
 // Along j (AXIS 1) or i (AXIS 0). Block TW x TY; each thread R consecutive outputs

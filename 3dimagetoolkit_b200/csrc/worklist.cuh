@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // ------------------------------------------------------------------ stage jobs
 // Each holds one volume's arguments of a kernel of kernels.cuh and runs its body.
 
-template <typename T, int N, int S, int TKT, int RKR, class Ld, class St>
+template <typename T, int N, int S, int TKT, int RKR, class Ld, class St, int RG>
 struct ConvKWinJob {
     Ld ld;
     St st;
@@ -69,7 +69,7 @@ struct ConvKWinJob {
     const T* taps;
     __device__ __forceinline__ void operator()(uint3 b, dim3 g, int) const
     {
-        conv_k_win_body<T, N, S, TKT, RKR, Ld, St>(b, g, ld, st, d, taps);
+        conv_k_win_body<T, N, S, TKT, RKR, Ld, St, RG>(b, g, ld, st, d, taps);
     }
 };
 
