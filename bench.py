@@ -610,15 +610,25 @@ def _oracle():
     return O
 
 
-def _ref_iterations(shape, maxiter, seed, threads):
+def _ref_fft(O, fft, threads) -> str:
+    """The FFT behind the reference's FFTW calls: scipy's pocketfft (multi-threaded) or
+    the in-tree FFT. Returns the one in use."""
+    if fft == "pocketfft" and O.use_pocketfft(threads):
+        return "scipy pocketfft behind the FFTW entry points (in place on the plan's output)"
+    O.use_pocketfft(None)
+    return "in-tree FP64 FFT behind the FFTW entry points"
+
+
+def _ref_iterations(shape, maxiter, seed, threads, fft="pocketfft"):
     """Runs the reference's own code (FP64) on the 256^3 workload for maxiter outer
     iterations with `threads` OpenMP threads; returns, per outer iteration after the
     first, its wall seconds, the seconds inside its Poisson step and inside FFTs, and
-    its sweeps."""
+    its sweeps, and the FFT used."""
     import numpy as np
 
     O = _oracle()
     O.set_threads(threads)
+    used = _ref_fft(O, fft, threads)
     pkg = importlib.import_module("3dimagetoolkit_b200")
     u0, phi0 = pkg.synth.config_volume("c2", seed=seed, dtype=np.float64)
     kw = dict(PARAMS)
@@ -629,9 +639,11 @@ def _ref_iterations(shape, maxiter, seed, threads):
     solve, fft = O.ref_last_step_profile()
     # iteration q runs from the end of step q-1 to the end of step q: the rest of
     # iteration q-1 (clamp, tolerance, Bregman, div) and the start and solve of q
-    return [{"seconds": float(ends[q] - ends[q - 1]), "solve": float(solve[q]),
-             "fft": float(fft[q] - fft[q - 1]), "sweeps": float(marks[q] - marks[q - 1])}
-            for q in range(1, len(ends))]
+    its = [{"seconds": float(ends[q] - ends[q - 1]), "solve": float(solve[q]),
+            "fft": float(fft[q] - fft[q - 1]), "sweeps": float(marks[q] - marks[q - 1])}
+           for q in range(1, len(ends))]
+    O.use_pocketfft(None)
+    return its, used
 
 
 def _fftw_probe() -> str:
@@ -649,6 +661,7 @@ def _fft_seconds(threads):
 
     O = _oracle()
     O.set_threads(threads)
+    O.use_pocketfft(None)
     rng = np.random.default_rng(0)
     x = rng.standard_normal((274, 274, 274)) + 1j * rng.standard_normal((274, 274, 274))
     O.ref_fft3d(x)
@@ -667,7 +680,7 @@ def _fft_seconds(threads):
     return shim, ducc
 
 
-def _ref_summary(its, threads, n):
+def _ref_summary(its, threads, n, used):
     """The reference arm's figures from measured outer iterations."""
     import numpy as np
 
@@ -686,6 +699,7 @@ def _ref_summary(its, threads, n):
         "seconds_per_sweep": per_sweep,
         "threads": threads,
         "fftw": _fftw_probe(),
+        "fft": used,
     }
     # The timed iterations are early ones; the full 100-iteration run (the GPU arm's
     # step) has its own sweep profile, recorded by the reference in the 256^3 fixture.
@@ -713,16 +727,16 @@ def _cpu_model() -> str:
 def cpu_baseline(args):
     threads = args.ref_threads or os.cpu_count()
     t0 = time.time()
-    its = _ref_iterations(SHAPE, 2, args.seed, threads)
+    its, used = _ref_iterations(SHAPE, 2, args.seed, threads, args.ref_fft)
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
-    summ = _ref_summary(its, threads, n)
+    summ = _ref_summary(its, threads, n, used)
     log(f"cpu baseline: {len(its)} timed iteration(s), {summ['seconds_per_iteration']:.2f} s each, "
         f"{time.time() - t0:.1f} s total")
     return {"value": summ["value"], "unit": UNIT, "cores": threads, "kind": "reference",
             "cpu_model": _cpu_model(), **{k: v for k, v in summ.items() if k != "value"},
-            "sample": "reference C++ (oracle/_ref: the reference headers, FFTW replaced by an "
-                      "in-tree FP64 FFT, VTK/GetPot by headless shims), T=double, 256^3, "
-                      "wall time of outer iteration 2 of 2 (setup and iteration 1 excluded)"}
+            "sample": "reference C++ (oracle/_ref: the reference headers compiled with headless "
+                      "VTK/GetPot shims; FFT as in `fft`), T=double, 256^3, wall time of outer "
+                      "iteration 2 of 2 (setup and iteration 1 excluded)"}
 
 
 def run_reference(args):
@@ -731,18 +745,12 @@ def run_reference(args):
         return
     threads = args.ref_threads or os.cpu_count()
     maxiter = 1 + args.warmup + args.steps
-    its = _ref_iterations(SHAPE, maxiter, args.seed, threads)
+    its, used = _ref_iterations(SHAPE, maxiter, args.seed, threads, args.ref_fft)
     timed = its[args.warmup:args.warmup + args.steps] if len(its) > args.warmup else its
     n = SHAPE[0] * SHAPE[1] * SHAPE[2]
-    summ = _ref_summary(timed, threads, n)
+    summ = _ref_summary(timed, threads, n, used)
     shim, ducc = _fft_seconds(threads)
-    fft_it = summ["breakdown_s_per_iteration"]["fft"]
     summ["fft_274cube_seconds"] = {"in_tree": shim, "scipy_pocketfft": ducc}
-    if ducc and "same_profile" in summ:
-        # the same iterations with every FFT at pocketfft's speed: what an FFTW-class
-        # library would give the reference, a bound on the in-tree FFT's share
-        per_it = summ["same_profile"]["seconds_per_iteration"] - fft_it * (1 - ducc / shim)
-        summ["same_profile"]["value_with_pocketfft_speed"] = n / per_it / 1e9
     value = summ.pop("value")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
@@ -771,6 +779,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-threads", type=int, default=0,
                     help="OpenMP threads of the reference's CPU code (default: all host cores)")
+    ap.add_argument("--ref-fft", default="pocketfft", choices=["pocketfft", "in-tree"],
+                    help="FFT behind the reference's FFTW calls (no FFTW on these hosts): scipy's "
+                         "pocketfft (default) or the in-tree FFT")
     ap.add_argument("--no-unet", action="store_true",
                     help="skip timing the library network behind the warm-start bound")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batch"],

@@ -282,6 +282,44 @@ def ref_fft_totals():
     return s.value, n.value
 
 
+_EXT_FFT = None  # the registered callback (kept alive while it is in use)
+
+
+def use_pocketfft(threads: int | None) -> bool:
+    """Serves the reference's fftw_execute calls with scipy's pocketfft (multi-threaded,
+    in place on the plan's output array) instead of the in-tree FFT; threads=None goes
+    back to the in-tree FFT. Returns False when scipy is missing. For timing the
+    reference: the checker's results use the in-tree FFT."""
+    global _EXT_FFT
+    L = ref_lib()
+    proto = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int)
+    L.im3d_fft_shim_set_external.argtypes = [proto]
+    if threads is None:
+        L.im3d_fft_shim_set_external(proto())
+        _EXT_FFT = None
+        return True
+    try:
+        import scipy.fft
+    except ImportError:
+        return False
+
+    def run(n0, n1, n2, data, sign):
+        n = n0 * n1 * n2
+        buf = (C.c_double * (2 * n)).from_address(data)
+        x = np.frombuffer(buf, dtype=np.complex128).reshape(n0, n1, n2)
+        if sign < 0:
+            y = scipy.fft.fftn(x, workers=threads, overwrite_x=True)
+        else:
+            y = scipy.fft.ifftn(x, norm="forward", workers=threads, overwrite_x=True)
+        if not np.shares_memory(x, y):
+            x[...] = y
+        return 0
+
+    _EXT_FFT = proto(run)
+    L.im3d_fft_shim_set_external(_EXT_FFT)
+    return True
+
+
 def set_threads(n: int) -> None:
     """OpenMP threads of the checker's and the reference's parallel regions started from
     the calling thread (omp_set_num_threads of the libgomp both libraries use)."""

@@ -15,6 +15,10 @@
  * recurrences), so the transform is accurate to a few ulp times log2(n).
  * A 3-D transform is three batches of 1-D transforms (axis 2 contiguous), parallel
  * over lines with OpenMP, as FFTW's threaded planner would run it.
+ *
+ * im3d_fft_shim_set_external() hands fftw_execute to another in-place transform: the
+ * timed CPU baseline registers scipy's pocketfft there (a tuned multi-threaded FFT, the
+ * closest stand-in for FFTW on these hosts), the checker keeps the in-tree transform.
  */
 #include "fftw3.h"
 
@@ -181,6 +185,11 @@ struct im3d_fft_plan_s {
 static int g_nthreads = 0;
 static double g_exec_seconds = 0;  // wall time spent in fftw_execute since the library loaded
 static long long g_exec_calls = 0;
+// An external in-place 3-D transform (unnormalised, sign as FFTW's) that serves
+// fftw_execute instead of the in-tree one when set (the CPU baseline registers a tuned
+// library's FFT here; the checker keeps the in-tree transform).
+typedef int (*im3d_fft_external_fn)(int n0, int n1, int n2, void* data, int sign);
+static im3d_fft_external_fn g_external = nullptr;
 
 static void execute_3d(im3d_fft_plan_s* p);
 
@@ -205,10 +214,25 @@ fftw_plan fftw_plan_dft_3d(int n0, int n1, int n2, fftw_complex* in, fftw_comple
 void fftw_execute(const fftw_plan pc)
 {
     const double t0 = omp_get_wtime();
-    execute_3d(pc);
+    if (g_external) {
+        const long total = (long)pc->n[0] * pc->n[1] * pc->n[2];
+        if (pc->out != pc->in) {
+            // out-of-place plan: the transform runs in place on out
+            const int nthreads = g_nthreads > 0 ? g_nthreads : omp_get_max_threads();
+            #pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long c = 0; c < total; c += 65536)
+                std::memcpy(pc->out + c, pc->in + c, sizeof(cplx) * std::min<long>(65536, total - c));
+        }
+        g_external(pc->n[0], pc->n[1], pc->n[2], pc->out, pc->sign);
+    } else {
+        execute_3d(pc);
+    }
     g_exec_seconds += omp_get_wtime() - t0;
     ++g_exec_calls;
 }
+
+/* Serve fftw_execute with an external transform (NULL: the in-tree one again). */
+void im3d_fft_shim_set_external(im3d_fft_external_fn fn) { g_external = fn; }
 
 /* Wall seconds spent in fftw_execute and the number of its calls since the library
  * loaded (the CPU baseline's FFT share of an outer iteration). */
