@@ -1980,10 +1980,11 @@ int wl_launch(im3d_ctx* ctx, const JobTable<Job>& t, const std::vector<int>& sel
     long long total = 0;
     for (int e = 0; e < wl.n; ++e) {
         const dim3 g = t.h[sel[e]].grid;
-        wl.first[e] = total;
+        wl.first[e] = (unsigned)total;
         total += (long long)g.x * g.y * g.z;
+        if (total > 0x7fffffffLL) break;
     }
-    wl.first[wl.n] = total;
+    wl.first[wl.n] = (unsigned)total;
     if (total > 0x7fffffffLL) return fail(ctx, IM3D_ERR_INVALID_ARG, "work list too large for one launch");
     auto kern = worklist_kernel<Job, THREADS, MINB>;
     IM3D_TRY(set_smem(ctx, kern, smem));
@@ -2295,7 +2296,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                     flags.push_back(C[q].beff2 < 0 ? 1 : 0);
                 }
             }
-            IM3D_TRY((wl_launch<Res, 256, 2>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
+            IM3D_TRY((wl_launch<Res, 256, 3>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
             IM3D_TRY(wl_finalize(ctx, fin_res_d, due, flags.data(), 1, SUM_RES2));
             IM3D_TRY(read_ctrls());
             std::vector<int> still;

@@ -1345,10 +1345,7 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
         const bool jint = j >= 1 && j <= d.ny - 2;
         const int lo = c.neu ? 0 : 1;
         const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
-        // every load of the NI planes is issued before the arithmetic (memory-level
-        // parallelism: the kernel waits on memory, not on its FP64 work)
-        VV o[NI + 2], bvv[NI], uvv[NI], ymv[NI], ypv[NI];
-        T exv[NI];
+        VV o[NI + 2];
 #pragma unroll
         for (int t = 0; t < NI + 2; ++t) {
             const int i = i0 - 1 + t;
@@ -1358,33 +1355,18 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
 #pragma unroll
         for (int t = 0; t < NI; ++t) {
             const int i = i0 + t;
+            if (i >= d.nx) break;
             const long long q = q0 + (long long)t * plane;
             const int par = (i + j + color) & 1;
-            bvv[t] = uvv[t] = ymv[t] = ypv[t] = VV{};
-            exv[t] = T(0);
-            if (i < d.nx) {
-                bvv[t] = *reinterpret_cast<const VV*>(bb + q);
-                uvv[t] = *reinterpret_cast<const VV*>(own + q);
-            }
-            if (jint && i >= 1 && i <= d.nx - 2) {
-                ymv[t] = *reinterpret_cast<const VV*>(oth + q - hz);
-                ypv[t] = *reinterpret_cast<const VV*>(oth + q + hz);
-                const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
-                if (e_ok) exv[t] = oth[par ? q + W : q - 1];
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < NI; ++t) {
-            const int i = i0 + t;
-            if (i >= d.nx) break;
-            const int par = (i + j + color) & 1;
             const bool rowint = jint && i >= 1 && i <= d.nx - 2;
-            const VV bv = bvv[t];
-            const VV uv = uvv[t];
+            const VV bv = *reinterpret_cast<const VV*>(bb + q);
+            const VV uv = *reinterpret_cast<const VV*>(own + q);
             if (rowint) {
-                const VV ym = ymv[t];
-                const VV yp = ypv[t];
-                const double extra = (double)exv[t];
+                const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
+                const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
+                const long long qe = par ? q + W : q - 1;
+                const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
+                const double extra = e_ok ? (double)oth[qe] : 0.0;
 #pragma unroll
                 for (int cc = 0; cc < W; ++cc) {
                     const int k = 2 * (m0 + cc) + par;

@@ -24,7 +24,7 @@ struct WorkList {
     int n;                                // entries (volumes) of this launch
     int vol[kMaxListVols];                // each entry's index into the job table
     int flag[kMaxListVols];               // a per-volume flag handed to the job
-    long long first[kMaxListVols + 1];    // first flat block of each entry; first[n] = total
+    unsigned first[kMaxListVols + 1];     // first flat block of each entry; first[n] = total (< 2^31)
 };
 
 template <class Job>
@@ -33,7 +33,7 @@ struct JobSlot {
     dim3 grid;  // the volume's own grid for this stage
 };
 
-__device__ __forceinline__ int worklist_entry(const WorkList& wl, long long b)
+__device__ __forceinline__ int worklist_entry(const WorkList& wl, unsigned b)
 {
     int lo = 0, hi = wl.n - 1;
     while (lo < hi) {
@@ -48,13 +48,15 @@ template <class Job, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
     worklist_kernel(const JobSlot<Job>* __restrict__ slots, const __grid_constant__ WorkList wl)
 {
-    const long long b = blockIdx.x;
+    // 32-bit index arithmetic only: a 64-bit division is a long software sequence, which
+    // every thread of the block would run
+    const unsigned b = blockIdx.x;
     const int e = worklist_entry(wl, b);
     const JobSlot<Job>* s = slots + wl.vol[e];
     const dim3 g = s->grid;
-    const long long r = b - wl.first[e];
-    const long long gxy = (long long)g.x * g.y;
-    const uint3 bi = make_uint3((unsigned)(r % g.x), (unsigned)((r / g.x) % g.y), (unsigned)(r / gxy));
+    const unsigned r = b - wl.first[e];
+    const unsigned q = r / g.x;
+    const uint3 bi = make_uint3(r - q * g.x, q % g.y, q / g.y);
     s->job(bi, g, wl.flag[e]);
 }
 
