@@ -686,15 +686,16 @@ int lex_sweep(im3d_ctx* ctx, T* r, const T* b, const Dims& d, const GsCoef<T>& c
 
 constexpr int kNI = 8;  // planes per thread of the scalar column-marching kernels
 constexpr int kNV = 2;  // planes per thread of the vectorised kernels (measured best on B200)
+constexpr int kNVres = 2;  // planes per thread of the residual check
 const dim3 kBlkVec(32, 4, 1);
 
-// vector groups of 16 bytes along the packed rows
+// vector groups of 16 bytes along the packed rows, ni planes per thread
 template <typename T>
-dim3 grid_vec_pk(const Dims& d, dim3 blk, int zmul = 1)
+dim3 grid_vec_pk(const Dims& d, dim3 blk, int zmul = 1, int ni = kNV)
 {
     const int groups = d.hz() / V16<T>::W;
     return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y,
-                ((d.nx + kNV - 1) / kNV) * zmul);
+                ((d.nx + ni - 1) / ni) * zmul);
 }
 
 template <typename T>
@@ -814,13 +815,13 @@ template <typename T>
 int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<T>& c,
              double* beff2, double* rel)
 {
-    const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2);
+    const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
     const int nvals = *beff2 < 0 ? 2 : 1;
     double* part = nullptr;
     IM3D_TRY(part_buf(ctx, grid, nvals, &part));
     ctx->residual_checks++;
     const int pf = prof_begin(ctx, "rb_residual");
-    rb_residual_vec_kernel<T, kNV><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
+    rb_residual_vec_kernel<T, kNVres><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
     prof_end(ctx, pf);
     IM3D_TRY(check_launch(ctx, "rb_residual"));
     IM3D_TRY(finalize(ctx, part, grid, nvals, SUM_RES2));
@@ -2028,6 +2029,10 @@ bool worklist_eligible(const im3d_rsfe_params* p, int nvol, const im3d_volume_de
     return true;
 }
 
+// Solve state of one subgroup of a work-list group (bytes of u and b_eff): about half
+// of the 126 MB L2
+constexpr size_t kSolveGroupBytes = 64ull << 20;
+
 // Per-volume loop counters of a work-list group.
 struct WlCount {
     bool done = false;
@@ -2086,7 +2091,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                                  dsc.nx, dsc.ny, dsc.nz, dsc.hx, dsc.hy, dsc.hz, p, nullptr, nullptr,
                                  nullptr, nullptr, nullptr);
         const Dims& d = V[q].d;
-        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2);
+        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
         const bool vec = d.nz % V16<T>::W == 0;
         const dim3 gc = vec ? grid_vec<T>(d, kBlkVec) : grid_col(d, kBlkVol);
         if (st == IM3D_OK)
@@ -2107,7 +2112,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
     constexpr int RB_MINB = sizeof(T) == 4 ? 8 : 1;
     using RbD = RbHalfJob<T, kNV, false, RB_MINB>;
     using RbN = RbHalfJob<T, kNV, true, 1>;
-    using Res = RbResidualJob<T, kNV>;
+    using Res = RbResidualJob<T, kNVres>;
     using ClV = ClampTolJob<T, kNV, true>;
     using ClS = ClampTolJob<T, kNI, false>;
     using BrV = BregmanJob<T, kNV, true>;
@@ -2168,7 +2173,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
             jrd[c].h.push_back({RbD{v.upk, v.bpk, d, v.coef, c, c}, gpk});
             jrn[c].h.push_back({RbN{v.upk, v.bpk, d, v.coef, c, c}, gpk});
         }
-        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2);
+        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
         jres.h.push_back({Res{v.upk, v.bpk, d, v.coef, part_res[q]}, gr});
         fin_res[q] = FinalizeJob{part_res[q], (long long)gr.x * gr.y * gr.z, ctrl[q].sum};
         vecrow[q] = d.nz % V16<T>::W == 0;
@@ -2275,55 +2280,72 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
             c.next = every > 0 ? every : (sched_first[q] > 0 ? sched_first[q] : 4);
         }
         const int pfs = prof_begin(ctx, "poisson_solve");
-        while (!solving.empty()) {
-            int k = maxs;
-            for (int q : solving) k = std::min(k, std::min(C[q].next, maxs) - C[q].s);
-            k = std::max(k, 1);
-            for (int i = 0; i < k; ++i)
-                for (int c = 0; c < 2; ++c) {
-                    if (neu)
-                        IM3D_TRY((wl_launch<RbN, 128, 1>(ctx, jrn[c], solving, nullptr, kBlkVec, 0, "rb_half", true)));
-                    else
-                        IM3D_TRY((wl_launch<RbD, 128, RB_MINB>(ctx, jrd[c], solving, nullptr, kBlkVec, 0, "rb_half",
-                                                               true)));
-                }
-            due.clear();
-            flags.clear();
-            for (int q : solving) {
-                C[q].s += k;
-                if (C[q].s >= C[q].next || C[q].s == maxs) {
-                    due.push_back(q);
-                    flags.push_back(C[q].beff2 < 0 ? 1 : 0);
-                }
+        // the volumes solve in subgroups whose solve state (u and b_eff, colour-packed)
+        // fits in L2 together, so that consecutive half-sweeps re-read it from L2 as a
+        // single volume's do; one launch per half-sweep covers the subgroup
+        std::vector<std::vector<int>> sub;
+        size_t sub_bytes = 0;
+        for (int q : act) {
+            const size_t b = (size_t)V[q].npk2 * 2 * sizeof(T);
+            if (sub.empty() || sub_bytes + b > kSolveGroupBytes) {
+                sub.emplace_back();
+                sub_bytes = 0;
             }
-            IM3D_TRY((wl_launch<Res, 256, 3>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
-            IM3D_TRY(wl_finalize(ctx, fin_res_d, due, flags.data(), 1, SUM_RES2));
-            IM3D_TRY(read_ctrls());
-            std::vector<int> still;
-            for (int q : solving) {
-                WlCount& c = C[q];
-                const bool checked = c.s >= c.next || c.s == maxs;
-                if (checked) {
-                    ++c.checks;
-                    const Ctrl& cb = ctx->wl_ctrl_h[q];
-                    if (c.beff2 < 0) c.beff2 = cb.sum[SUM_BEFF2];
-                    const double rr = cb.sum[SUM_RES2];
-                    const double r = c.beff2 > 0 ? std::sqrt(rr) / std::sqrt(c.beff2) : std::sqrt(rr);
-                    c.rel = r;
-                    if (r <= p->gs_rel_res_tol) {
-                        c.conv = true;
-                        continue;
+            sub.back().push_back(q);
+            sub_bytes += b;
+        }
+        for (const auto& grp : sub) {
+            solving = grp;
+            while (!solving.empty()) {
+                int k = maxs;
+                for (int q : solving) k = std::min(k, std::min(C[q].next, maxs) - C[q].s);
+                k = std::max(k, 1);
+                for (int i = 0; i < k; ++i)
+                    for (int c = 0; c < 2; ++c) {
+                        if (neu)
+                            IM3D_TRY((wl_launch<RbN, 128, 1>(ctx, jrn[c], solving, nullptr, kBlkVec, 0, "rb_half", true)));
+                        else
+                            IM3D_TRY((wl_launch<RbD, 128, RB_MINB>(ctx, jrd[c], solving, nullptr, kBlkVec, 0, "rb_half",
+                                                                   true)));
                     }
-                    if (c.s >= maxs) continue;  // not converged
-                    c.next = next_check(c.s, r, c.s_prev, c.r_prev, p->gs_rel_res_tol, every, sched_rate[q],
-                                        &c.rate_used);
-                    if (c.next > maxs) c.next = maxs;
-                    c.s_prev = c.s;
-                    c.r_prev = r;
+                due.clear();
+                flags.clear();
+                for (int q : solving) {
+                    C[q].s += k;
+                    if (C[q].s >= C[q].next || C[q].s == maxs) {
+                        due.push_back(q);
+                        flags.push_back(C[q].beff2 < 0 ? 1 : 0);
+                    }
                 }
-                still.push_back(q);
+                IM3D_TRY((wl_launch<Res, 256, 3>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
+                IM3D_TRY(wl_finalize(ctx, fin_res_d, due, flags.data(), 1, SUM_RES2));
+                IM3D_TRY(read_ctrls());
+                std::vector<int> still;
+                for (int q : solving) {
+                    WlCount& c = C[q];
+                    const bool checked = c.s >= c.next || c.s == maxs;
+                    if (checked) {
+                        ++c.checks;
+                        const Ctrl& cb = ctx->wl_ctrl_h[q];
+                        if (c.beff2 < 0) c.beff2 = cb.sum[SUM_BEFF2];
+                        const double rr = cb.sum[SUM_RES2];
+                        const double r = c.beff2 > 0 ? std::sqrt(rr) / std::sqrt(c.beff2) : std::sqrt(rr);
+                        c.rel = r;
+                        if (r <= p->gs_rel_res_tol) {
+                            c.conv = true;
+                            continue;
+                        }
+                        if (c.s >= maxs) continue;  // not converged
+                        c.next = next_check(c.s, r, c.s_prev, c.r_prev, p->gs_rel_res_tol, every, sched_rate[q],
+                                            &c.rate_used);
+                        if (c.next > maxs) c.next = maxs;
+                        c.s_prev = c.s;
+                        c.r_prev = r;
+                    }
+                    still.push_back(q);
+                }
+                solving.swap(still);
             }
-            solving.swap(still);
         }
         prof_end(ctx, pfs);
         for (int q : act) {
@@ -2340,7 +2362,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         // clamp and tolerance, then the Bregman update and div(d - b)
         split(act, sv, ss);
         IM3D_TRY((wl_launch<ClV, 256, 4>(ctx, jclv, sv, nullptr, kBlkVec, 0, "clamp_tol")));
-        IM3D_TRY((wl_launch<ClS, 256, 1>(ctx, jcls, ss, nullptr, kBlkVol, 0, "clamp_tol")));
+        IM3D_TRY((wl_launch<ClS, 256, 1>(ctx, jcls, ss, nullptr, kBlkVol, 0, "clamp_tol_columns")));
         IM3D_TRY(wl_finalize(ctx, fin_cl_d, act, nullptr, 2, SUM_DPHI2));
         IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->wl_ctrl_h, ctrl, nv * sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
         IM3D_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
@@ -2356,9 +2378,9 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         }
         split(upd, sv, ss);
         IM3D_TRY((wl_launch<BrV, 256, 2>(ctx, jbrv, sv, nullptr, kBlkVec, 0, "bregman")));
-        IM3D_TRY((wl_launch<BrS, 256, 1>(ctx, jbrs, ss, nullptr, kBlkVol, 0, "bregman")));
+        IM3D_TRY((wl_launch<BrS, 256, 1>(ctx, jbrs, ss, nullptr, kBlkVol, 0, "bregman_columns")));
         IM3D_TRY((wl_launch<DvV, 256, 3>(ctx, jdvv, sv, nullptr, kBlkVec, 0, "div")));
-        IM3D_TRY((wl_launch<DvS, 256, 1>(ctx, jdvs, ss, nullptr, kBlkVol, 0, "div")));
+        IM3D_TRY((wl_launch<DvS, 256, 1>(ctx, jdvs, ss, nullptr, kBlkVol, 0, "div_columns")));
         if (cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) IM3D_TRY(sync(ctx));
         for (int q : act) {
             const Ctrl& cb = ctx->wl_ctrl_h[q];

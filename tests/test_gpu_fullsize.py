@@ -1,18 +1,15 @@
-"""GPU: the benchmark workloads at full size, through properties that do not need the
-CPU checker (which would take hours at these sizes):
+"""GPU: the benchmark workloads at full size.
 
-- the FP32 path against the FP64 path on the same seed and solve tolerance. After 10
-  outer iterations at 256^3 the fields meet the per-field bars of the workload (u, f1,
-  f2 relative L2 <= 1e-5); over a full run the FP32 rounding of each outer iteration
-  (~2e-7) accumulates, since the outer iteration does not damp earlier errors, so the
-  full runs are held to the segmentation bars (sign(phi - 0.5) agreement >= 99.9 %, Dice >=
-  0.999) and to bounds on the field drift about three times what was measured on B200
-  (256^3, 100 it.: u 9.2e-5, f1 2.0e-5, f2 2.9e-5; 512x512x320, 200 it.: u 1.8e-3, f1
-  5.0e-4, f2 4.2e-4, Dice 0.99967; an FP64 run at the same tolerance is itself 1.9e-5
-  from a fully converged one at 256^3); the FP64 path is checked against the checker at
-  smaller sizes;
-- every Poisson solve reached the relative residual it was asked for;
-- a second run gives bit-identical results (deterministic reductions and sweeps)."""
+- Against the reference's own run of the 256^3 workload (tests/golden/rsfe_c2_256_ref.npz,
+  written by tests/golden/make_fullsize_fixture.py through oracle/_ref): the FP64 path
+  reproduces its iteration, sweep and check counts and its segmentation bit for bit, and
+  the FP32 path meets the per-field bars of the workload (u, f1, f2 relative L2 <= 1e-5,
+  sign agreement and Dice >= 0.9999; measured on B200: u 4.4e-6, f1 5.9e-7, f2 4.6e-7,
+  the same segmentation bit for bit).
+- The FP32 path against the FP64 path on the same seed and solve tolerance, at 256^3 and
+  at 512x512x320 (the CPU checker would take hours there).
+- Every Poisson solve reached the relative residual it was asked for, and a second run
+  gives bit-identical results (deterministic reductions and sweeps)."""
 import hashlib
 import json
 import os
@@ -27,15 +24,15 @@ pytestmark = pytest.mark.gpu
 # the reference's own code run once on the 256^3 workload (tests/golden/make_fullsize_fixture.py)
 FIXTURE = os.path.join(ROOT, "tests", "golden", "rsfe_c2_256_ref.npz")
 LATTICE = (slice(1, None, 4), slice(2, None, 4), slice(3, None, 4))
-# relative L2 bounds of the FP32 fields against the reference run (256^3, 100 outer
-# iterations)
-FP32_BOUNDS = {"u": 3e-4, "f1": 1e-4, "f2": 1e-4}
+# relative L2 bars of the FP32 fields against the reference run (256^3, 100 outer
+# iterations): the workload's per-field bar
+FP32_BOUNDS = {"u": 1e-5, "f1": 1e-5, "f2": 1e-5}
 
 PARAMS = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, bc=2, tol=0.0,
               gs_rel_res_tol=1e-6, gs_max_sweeps=1000)
 # workload, outer iterations, bounds on the relative L2 of (u, f1, f2)
 CASES = [("c2", dict(maxiter=10), (1e-5, 1e-5, 1e-5)),
-         ("c2", dict(maxiter=100), (3e-4, 1e-4, 1e-4)),
+         ("c2", dict(maxiter=100), (1e-5, 1e-5, 1e-5)),
          ("c3", dict(maxiter=200, sigma=4.0), (5e-3, 1.5e-3, 1.5e-3))]
 
 
@@ -105,9 +102,9 @@ def test_fp32_against_the_reference_at_256(ctx, pkg):
     assert r["stats"]["not_converged"] == 0
     ref_in = np.unpackbits(fx["inside_bits"])[: u0.size].astype(bool)
     mine = (r["phi"] > 0.5).ravel()
-    assert np.mean(ref_in == mine) >= 0.999
+    assert np.mean(ref_in == mine) >= 0.9999
     dice = 2.0 * np.logical_and(ref_in, mine).sum() / (ref_in.sum() + mine.sum())
-    assert dice >= 0.999
+    assert dice >= 0.9999
     for key, bound in FP32_BOUNDS.items():
         got = rel(r[key][LATTICE].astype(np.float64), fx[key + "_lattice"].astype(np.float64))
         assert got <= bound, (key, got)

@@ -9,9 +9,8 @@ roundings emulated where it rounds).
   wider tensor and two samples.
 * The network's forward pass: every layer rounds its output to BF16, so a sum whose
   order differs lands on the other side of a rounding now and then, and the flips
-  compound over the 13 layers: the checker itself, summing in FP32 and in FP64, differs
-  by a few 1e-3. The GPU output must lie within three times that spread (and 2e-3) of
-  the FP64-summed checker.
+  compound over the 13 layers. The GPU output must lie within 1e-2 of the FP64-summed
+  checker with the BF16 roundings, and nearer to it than the checker without them is.
 * Its gradients (the tcgen05 data- and weight-gradient kernels, the pooling, transposed
   convolution and output-layer kernels): per parameter tensor relative L2 <= 3e-2 and
   cosine >= 0.999 against torch autograd; the loss to 1e-3.
@@ -81,11 +80,17 @@ def test_network_forward_matches_cpu(pkg, ctx, shape, nsamp):
     with net:
         y = net.forward(x)
     ps = R.unflatten(flat)
-    want32 = R.forward(torch.tensor(x), ps, emulate_bf16=True)[:, 0].detach().numpy()
     ps64 = {k: v.double() for k, v in ps.items()}
-    want = R.forward(torch.tensor(x, dtype=torch.float64), ps64, emulate_bf16=True)[:, 0].detach().numpy()
-    spread = rel(want32, want)
-    assert rel(y, want) <= max(3.0 * spread, 2e-3), (rel(y, want), spread)
+    x64 = torch.tensor(x, dtype=torch.float64)
+    want = R.forward(x64, ps64, emulate_bf16=True)[:, 0].detach().numpy()
+    plain = R.forward(x64, ps64, emulate_bf16=False)[:, 0].detach().numpy()
+    # Each BF16 rounding of an activation near a rounding boundary flips with the order
+    # of the FP32 sums before it (one BF16 ulp, 0.4 %), and the flips propagate through
+    # the layers, so the GPU and the checker differ by a fraction of the BF16 effect
+    # itself (measured on B200: 0.02-0.63 %, against a BF16 effect of 0.8-0.9 %).
+    got = rel(y, want)
+    assert got <= 1e-2, got
+    assert got < rel(plain, want), (got, rel(plain, want))
 
 
 @pytest.mark.parametrize("shape, nsamp", [((8, 8, 64), 1), ((4, 4, 128), 2)])
