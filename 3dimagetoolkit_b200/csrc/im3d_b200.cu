@@ -73,6 +73,7 @@ struct im3d_ctx {
     std::vector<im3d_ctx*> vols;
     Ctrl* wl_ctrl_h = nullptr;
     int wl_ctrl_cap = 0;
+    cudaEvent_t wl_ev[2] = {nullptr, nullptr};  // work-list solve phase: start, this worker done
     int batch_mode = IM3D_BATCH_AUTO;
     int num_sms = 148;
     int ifit_chunks = 0;  // i chunks of the marching fit stage (0: cost model)
@@ -1941,6 +1942,21 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                double hx, double hy, double hz, const im3d_rsfe_params* p, T* phi_user, T* u_user,
                T* f1_user, T* f2_user, im3d_rsfe_stats* stats);
 
+// Worker contexts of the batched entry points: own stream and buffers each.
+int ensure_workers(im3d_ctx* ctx, int n)
+{
+    while ((int)ctx->workers.size() < n) {
+        im3d_ctx* w = nullptr;
+        const int st = im3d_ctx_create(ctx->device, &w);
+        if (st != IM3D_OK) return fail(ctx, st, "cannot create a worker context");
+        w->mem_limit = ctx->mem_limit;
+        w->ifit_chunks = ctx->ifit_chunks;
+        ctx->workers.push_back(w);
+    }
+    for (im3d_ctx* w : ctx->workers) w->prof = 0;
+    return IM3D_OK;
+}
+
 // ------------------------------------------------------------ work-list batch
 // Volumes of a group advance their outer iterations together; each stage of the loop
 // is one launch over every volume that runs it (worklist.cuh).
@@ -2047,10 +2063,11 @@ struct WlCount {
 
 template <typename T, int S>
 int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume_desc* vols,
-                   const im3d_rsfe_params* p, im3d_rsfe_stats* stats, double* latency_ms,
+                   const im3d_rsfe_params* p, int streams, im3d_rsfe_stats* stats, double* latency_ms,
                    std::chrono::steady_clock::time_point t_start)
 {
     const int nv = (int)ids.size();
+    IM3D_TRY(ensure_workers(ctx, streams));
     const bool neu = p->bc == IM3D_BC_NEU;
     while ((int)ctx->vols.size() < nv) {
         im3d_ctx* v = nullptr;
@@ -2221,10 +2238,6 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         sched_rate[q] = V[q].sched_rate;
         init_vars[q] = V[q].init_variables;
     }
-    auto read_ctrls = [&]() -> int {
-        IM3D_CUDA(ctx, cudaMemcpyAsync(ctx->wl_ctrl_h, ctrl, nv * sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
-        return sync(ctx);
-    };
     auto split = [&](const std::vector<int>& sel, std::vector<int>& a, std::vector<int>& b) {
         a.clear();
         b.clear();
@@ -2233,7 +2246,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
     const size_t smem_k4 = k_win_smem<T, 4, S>(), smem_k2 = k_win_smem<T, 2, S>();
     const size_t smem_s4 = s_win_smem<T, 4, S>(), smem_s2 = s_win_smem<T, 2, S>();
     const dim3 blk_k(kKwT, kKwR), blk_s(TW, TY);
-    std::vector<int> act, solving, due, flags, sv, ss;
+    std::vector<int> act, sv, ss;
     // a volume whose loop would not start (maxiter < 1) returns its initial level set
     for (int q = 0; q < nv; ++q)
         if (!(tol[q] > p->tol) || p->maxiter < 1) {
@@ -2267,7 +2280,6 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         // (next_check) asks for one
         const int maxs = std::max(p->gs_max_sweeps, 1);
         const int every = std::max(p->gs_check_every, 0);
-        solving = act;
         for (int q : act) {
             WlCount& c = C[q];
             c.s = 0;
@@ -2294,8 +2306,13 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
             sub.back().push_back(q);
             sub_bytes += b;
         }
-        for (const auto& grp : sub) {
-            solving = grp;
+        // one subgroup's solves on the context `sc` (its stream): the half-sweeps of its
+        // unconverged volumes in one launch each, a residual check of each volume on its
+        // own schedule; the volumes of a subgroup have consecutive indices, so their
+        // control blocks are one range
+        auto solve_group = [&](im3d_ctx* sc, const std::vector<int>& grp) -> int {
+            std::vector<int> solving = grp, due, flags, still;
+            const int q0 = grp.front(), q1 = grp.back() + 1;
             while (!solving.empty()) {
                 int k = maxs;
                 for (int q : solving) k = std::min(k, std::min(C[q].next, maxs) - C[q].s);
@@ -2303,9 +2320,9 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                 for (int i = 0; i < k; ++i)
                     for (int c = 0; c < 2; ++c) {
                         if (neu)
-                            IM3D_TRY((wl_launch<RbN, 128, 1>(ctx, jrn[c], solving, nullptr, kBlkVec, 0, "rb_half", true)));
+                            IM3D_TRY((wl_launch<RbN, 128, 1>(sc, jrn[c], solving, nullptr, kBlkVec, 0, "rb_half", true)));
                         else
-                            IM3D_TRY((wl_launch<RbD, 128, RB_MINB>(ctx, jrd[c], solving, nullptr, kBlkVec, 0, "rb_half",
+                            IM3D_TRY((wl_launch<RbD, 128, RB_MINB>(sc, jrd[c], solving, nullptr, kBlkVec, 0, "rb_half",
                                                                    true)));
                     }
                 due.clear();
@@ -2317,10 +2334,12 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                         flags.push_back(C[q].beff2 < 0 ? 1 : 0);
                     }
                 }
-                IM3D_TRY((wl_launch<Res, 256, 3>(ctx, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
-                IM3D_TRY(wl_finalize(ctx, fin_res_d, due, flags.data(), 1, SUM_RES2));
-                IM3D_TRY(read_ctrls());
-                std::vector<int> still;
+                IM3D_TRY((wl_launch<Res, 256, 3>(sc, jres, due, flags.data(), kBlkVec, 0, "rb_residual")));
+                IM3D_TRY(wl_finalize(sc, fin_res_d, due, flags.data(), 1, SUM_RES2));
+                IM3D_CUDA(sc, cudaMemcpyAsync(ctx->wl_ctrl_h + q0, ctrl + q0, (q1 - q0) * sizeof(Ctrl),
+                                              cudaMemcpyDeviceToHost, sc->stream));
+                IM3D_CUDA(sc, cudaStreamSynchronize(sc->stream));
+                still.clear();
                 for (int q : solving) {
                     WlCount& c = C[q];
                     const bool checked = c.s >= c.next || c.s == maxs;
@@ -2346,6 +2365,41 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                 }
                 solving.swap(still);
             }
+            return IM3D_OK;
+        };
+        // the subgroups run concurrently on the worker streams, each after the forcing
+        // terms are written (so a worker's residual round trips overlap the others'
+        // sweeps); the loop's stream then waits for all of them
+        const int nw = std::min<int>(streams, (int)sub.size());
+        IM3D_CUDA(ctx, cudaEventRecord(ctx->wl_ev[0], ctx->stream));
+        std::atomic<int> next_sub(0);
+        std::vector<int> wst(nw, IM3D_OK);
+        auto work = [&](int w) {
+            im3d_ctx* wc = ctx->workers[w];
+            cudaSetDevice(wc->device);
+            wc->err.clear();
+            if (cudaStreamWaitEvent(wc->stream, ctx->wl_ev[0], 0) != cudaSuccess) {
+                wst[w] = fail(wc, IM3D_ERR_CUDA, "cannot order a worker stream after the forcing terms");
+                return;
+            }
+            for (int g = next_sub++; g < (int)sub.size(); g = next_sub++) {
+                wst[w] = solve_group(wc, sub[g]);
+                if (wst[w] != IM3D_OK) break;
+            }
+            cudaEventRecord(wc->wl_ev[1], wc->stream);
+        };
+        {
+            std::vector<std::thread> pool;
+            for (int w = 1; w < nw; ++w) pool.emplace_back(work, w);
+            work(0);
+            for (auto& th : pool) th.join();
+        }
+        cudaSetDevice(ctx->device);
+        for (int w = 0; w < nw; ++w) {
+            ctx->launches += ctx->workers[w]->launches;
+            ctx->workers[w]->launches = 0;
+            if (wst[w] != IM3D_OK) return fail(ctx, wst[w], ctx->workers[w]->err);
+            IM3D_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->workers[w]->wl_ev[1], 0));
         }
         prof_end(ctx, pfs);
         for (int q : act) {
@@ -2425,7 +2479,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
 // Work-list batch: groups of up to kMaxListVols volumes, largest first.
 template <typename T>
 int rsfe_apply_worklist(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols, const im3d_rsfe_params* p,
-                        int nh, im3d_rsfe_stats* stats, double* latency_ms)
+                        int nh, int streams, im3d_rsfe_stats* stats, double* latency_ms)
 {
     std::vector<int> order(nvol);
     for (int v = 0; v < nvol; ++v) order[v] = v;
@@ -2435,8 +2489,8 @@ int rsfe_apply_worklist(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols, c
     const auto t0 = std::chrono::steady_clock::now();
     for (int g0 = 0; g0 < nvol; g0 += kMaxListVols) {
         const std::vector<int> ids(order.begin() + g0, order.begin() + std::min(nvol, g0 + kMaxListVols));
-        if (nh == 19) IM3D_TRY((worklist_group<T, 9>(ctx, ids, vols, p, stats, latency_ms, t0)));
-        else IM3D_TRY((worklist_group<T, 12>(ctx, ids, vols, p, stats, latency_ms, t0)));
+        if (nh == 19) IM3D_TRY((worklist_group<T, 9>(ctx, ids, vols, p, streams, stats, latency_ms, t0)));
+        else IM3D_TRY((worklist_group<T, 12>(ctx, ids, vols, p, streams, stats, latency_ms, t0)));
     }
     return IM3D_OK;
 }
@@ -2450,6 +2504,8 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
 {
     if (nvol < 0 || (nvol > 0 && !vols) || !p) return fail(ctx, IM3D_ERR_INVALID_ARG, "bad batch");
     if (nvol == 0) return IM3D_OK;
+    if (streams <= 0) streams = 4;
+    if (streams > 32) streams = 32;
     if (ctx->batch_mode != IM3D_BATCH_STREAMS) {
         // the work list runs valid volumes only; otherwise the stream queue reports each
         // bad volume and segments the others
@@ -2462,7 +2518,7 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
         }
         int nh = 0;
         if (st == IM3D_OK && worklist_eligible<T>(p, nvol, vols, &nh))
-            return rsfe_apply_worklist<T>(ctx, nvol, vols, p, nh, stats, latency_ms);
+            return rsfe_apply_worklist<T>(ctx, nvol, vols, p, nh, streams, stats, latency_ms);
         if (ctx->batch_mode == IM3D_BATCH_WORKLIST) {
             if (st != IM3D_OK) return st;
             return fail(ctx, IM3D_ERR_UNSUPPORTED, "the work-list batch needs a residual solve with omega 1, "
@@ -2471,17 +2527,8 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
         }
         ctx->err.clear();
     }
-    if (streams <= 0) streams = 4;
     if (streams > nvol) streams = nvol;
-    if (streams > 32) streams = 32;
-    while ((int)ctx->workers.size() < streams) {
-        im3d_ctx* w = nullptr;
-        const int st = im3d_ctx_create(ctx->device, &w);
-        if (st != IM3D_OK) return fail(ctx, st, "cannot create a worker context");
-        w->mem_limit = ctx->mem_limit;
-        w->ifit_chunks = ctx->ifit_chunks;
-        ctx->workers.push_back(w);
-    }
+    IM3D_TRY(ensure_workers(ctx, streams));
     std::vector<int> order(nvol);
     for (int v = 0; v < nvol; ++v) order[v] = v;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -2590,6 +2637,7 @@ int im3d_ctx_create(int device, im3d_ctx** out)
     }
     for (int q = 0; q < 3; ++q) cudaEventCreate(&ctx->ev[q]);
     cudaEventCreateWithFlags(&ctx->ev[3], cudaEventDisableTiming);
+    for (auto& e : ctx->wl_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     ctx->stream = ctx->own_stream;
     ctx->num_sms = prop.multiProcessorCount;
     *out = ctx;
@@ -2612,6 +2660,8 @@ int im3d_ctx_destroy(im3d_ctx* ctx)
     if (ctx->ctrl_d) cudaFree(ctx->ctrl_d);
     if (ctx->ctrl_h) cudaFreeHost(ctx->ctrl_h);
     for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->wl_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;

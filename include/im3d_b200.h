@@ -398,12 +398,13 @@ typedef struct im3d_volume_desc {
 /* Segments nvol volumes with the same parameters, in one of two ways
  * (IM3D_OPT_BATCH_MODE):
  *  - the work list: groups of up to 64 volumes, largest first, advance their outer
- *    iterations together, and each stage of the loop is ONE launch over the blocks of
- *    every volume of the group that still runs it (each Poisson half-sweep over the
- *    volumes whose solve has not converged, each residual check over those due for
- *    one). Runs when the Poisson step is solved to a residual (gs_rel_res_tol > 0,
- *    omega 1), the Gaussian has 19 or 25 taps on every axis of every volume and no
- *    connected-component extraction is asked for; `streams` is then unused.
+ *    iterations together; each convolution, clamp, Bregman and div stage is ONE
+ *    launch over the blocks of every volume of the group, and the Poisson solves run
+ *    in L2-sized subgroups of volumes (one launch per half-sweep and per residual
+ *    check of a subgroup) on `streams` concurrent worker streams (0 = 4). Runs when
+ *    the Poisson step is solved to a residual (gs_rel_res_tol > 0, omega 1), the
+ *    Gaussian has 19 or 25 taps on every axis of every volume and no
+ *    connected-component extraction is asked for.
  *  - the stream queue: volumes are taken largest first from a shared queue by
  *    `streams` workers (0 = 4), each running whole segmentations on its own CUDA
  *    stream with its own device buffers, so small volumes overlap on the GPU.
