@@ -21,6 +21,26 @@ def test_fft_shim_matches_numpy(O):
         assert rel(O.ref_fft3d(x, +1), np.fft.ifftn(x) * x.size) < 1e-14
 
 
+def test_pocketfft_behind_the_shim_matches(O):
+    """The CPU baseline serves the reference's FFTW calls with scipy's pocketfft: the
+    same transforms (and the same reference convolution) as the in-tree FFT."""
+    _need_ref(O)
+    pytest.importorskip("scipy")
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((20, 19, 13)) + 1j * rng.standard_normal((20, 19, 13))
+    v = rng.random((18, 20, 22))
+    a_fwd, a_bwd = O.ref_fft3d(x, -1), O.ref_fft3d(x, +1)
+    a_conv = O.ref_gauss_filter(v, 2.0)
+    try:
+        assert O.use_pocketfft(2)
+        assert rel(O.ref_fft3d(x, -1), a_fwd) < 1e-14
+        assert rel(O.ref_fft3d(x, +1), a_bwd) < 1e-14
+        assert rel(O.ref_gauss_filter(v, 2.0), a_conv) < 1e-13
+    finally:
+        O.use_pocketfft(None)
+    assert np.array_equal(O.ref_fft3d(x, -1), a_fwd)
+
+
 @pytest.mark.parametrize("h", [(1.0, 1.0, 1.0), (0.8, 1.1, 1.3)])
 @pytest.mark.parametrize("gpa", [False, True])
 def test_separable_conv_equals_reference_fft_and_direct(O, h, gpa):
