@@ -706,10 +706,13 @@ dim3 grid_vec(const Dims& d, dim3 blk)
     return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNV - 1) / kNV);
 }
 
-dim3 grid_col(const Dims& d, dim3 blk)
+dim3 grid_col(const Dims& d, dim3 blk, int ni = kNI)
 {
-    return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNI - 1) / kNI);
+    return dim3((d.nz + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + ni - 1) / ni);
 }
+
+// planes per thread of the column Bregman kernel (it holds every load of its planes)
+constexpr int kNIbr = 2;
 
 // Launch as a programmatic dependent of the previous kernel on the stream: the kernel
 // must begin with griddepcontrol.wait (rb_half_vec_kernel does), which holds it until
@@ -1545,7 +1548,7 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
                 bregman_vec_kernel<T, kNV><<<grid_vec<T>(d, kBlkVec), kBlkVec, 0, ctx->stream>>>(
                     phi_new, b3, dmb, g, d, hx, hy, hz);
             else
-                bregman_kernel<T, kNI><<<grid_col(d, kBlkVol), kBlkVol, 0, ctx->stream>>>(
+                bregman_kernel<T, kNIbr><<<grid_col(d, kBlkVol, kNIbr), kBlkVol, 0, ctx->stream>>>(
                     phi_new, b3, dmb, g, d, hx, hy, hz);
             prof_end(ctx, pf);
             IM3D_TRY(check_launch(ctx, "bregman"));
@@ -2133,7 +2136,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
     using ClV = ClampTolJob<T, kNV, true>;
     using ClS = ClampTolJob<T, kNI, false>;
     using BrV = BregmanJob<T, kNV, true>;
-    using BrS = BregmanJob<T, kNI, false>;
+    using BrS = BregmanJob<T, kNIbr, false>;
     using DvV = DivJob<T, kNV, true>;
     using DvS = DivJob<T, 0, false>;
     JobTable<KHeav> jk;
@@ -2200,7 +2203,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         const dim3 gcl = vecrow[q] ? gv : gcol;
         fin_cl[q] = FinalizeJob{part_cl[q], (long long)gcl.x * gcl.y * gcl.z, ctrl[q].sum};
         jbrv.h.push_back({BrV{v.phi, v.b3, v.dmb, v.g, d, hx, hy, hz}, gv});
-        jbrs.h.push_back({BrS{v.phi, v.b3, v.dmb, v.g, d, hx, hy, hz}, gcol});
+        jbrs.h.push_back({BrS{v.phi, v.b3, v.dmb, v.g, d, hx, hy, hz}, grid_col(d, kBlkVol, kNIbr)});
         jdvv.h.push_back({DvV{v.dmb, v.divdb, d, hx, hy, hz}, gv});
         jdvs.h.push_back({DvS{v.dmb, v.divdb, d, hx, hy, hz}, gvol});
     }

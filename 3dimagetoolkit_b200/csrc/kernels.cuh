@@ -1421,23 +1421,37 @@ __device__ __forceinline__ void clamp_tol_body(const uint3 blockIdx, const dim3 
     const int i0 = blockIdx.z * NI;
     double s_d = 0, s_o = 0;
     if (k < d.nz && j < d.ny) {
-        const int i_end = min(i0 + NI, d.nx);
+        const int cnt = min(NI, d.nx - i0);
         const long long plane = (long long)d.ny * d.nz;
         const long long pplane = (long long)d.ny * d.hz();
-        long long p = d.idx(i0, j, k);
-        long long pq = d.pidx(i0, j, k);
+        const long long p0 = d.idx(i0, j, k);
+        const long long pq0 = d.pidx(i0, j, k);
         const long long npk = pplane * d.nx;
-        for (int i = i0; i < i_end; ++i, p += plane, pq += pplane) {
-            const T uv = PACKED ? u[pq + (((i + j + k) & 1) ? npk : 0)] : u[p];
-            if (u_out) u_out[p] = uv;
-            T v = uv;
-            if (v < a0) v = a0;
-            else if (v > b0) v = b0;
-            const T old = phi[p];
-            phi[p] = v;
-            const double df = (double)v - (double)old;
-            s_d += df * df;
-            s_o += (double)old * (double)old;
+        // every load of the NI planes before the first store: a store to phi would
+        // otherwise hold the next plane's loads back (one memory round trip per plane)
+        T uv[NI], ov[NI];
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            if (t < cnt) {
+                const long long p = p0 + t * plane;
+                uv[t] = PACKED ? u[pq0 + t * pplane + (((i0 + t + j + k) & 1) ? npk : 0)] : u[p];
+                ov[t] = phi[p];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+            if (t < cnt) {
+                const long long p = p0 + t * plane;
+                if (u_out) u_out[p] = uv[t];
+                T v = uv[t];
+                if (v < a0) v = a0;
+                else if (v > b0) v = b0;
+                const T old = ov[t];
+                phi[p] = v;
+                const double df = (double)v - (double)old;
+                s_d += df * df;
+                s_o += (double)old * (double)old;
+            }
         }
     }
     block_sum2_store(s_d, s_o, part, block_linear_id(blockIdx, gridDim), grid_blocks(gridDim));
@@ -1460,30 +1474,73 @@ __device__ __forceinline__ void bregman_body(const uint3 blockIdx, const dim3 gr
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i0 = blockIdx.z * NI;
     if (k >= d.nz || j >= d.ny) return;
-    const int i_end = min(i0 + NI, d.nx);
+    const int cnt = min(NI, d.nx - i0);
     const long long plane = (long long)d.ny * d.nz;
     const long long n = d.n();
     const long long sy = d.nz;
-    long long p = d.idx(i0, j, k);
-    T fm = i0 >= 1 ? phi[p - plane] : T(0);
-    T f0 = phi[p];
+    const long long p0 = d.idx(i0, j, k);
     const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
-    for (int i = i0; i < i_end; ++i, p += plane) {
-        const T fp = i + 1 < d.nx ? phi[p + plane] : T(0);
+    // Every load of the NI planes is issued before the first store (the stores to b3
+    // and dmb would otherwise hold the next plane's loads back): phi along i for planes
+    // i0-1 .. i0+NI (and the second one-sided point on an i face), the j and k
+    // neighbours of each plane, g and the three components of b.
+    T fi[NI + 2], fi2[NI], fjm[NI], fjp[NI], fkm[NI], fkp[NI], gv[NI], bv0[NI][3];
+#pragma unroll
+    for (int t = 0; t < NI + 2; ++t) {
+        const int i = i0 - 1 + t;
+        fi[t] = (i >= 0 && i < d.nx && t <= cnt + 1) ? phi[p0 + (long long)(t - 1) * plane] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        if (t >= cnt) break;
+        const int i = i0 + t;
+        const long long p = p0 + (long long)t * plane;
+        fi2[t] = i == 0 ? phi[p + 2 * plane] : (i == d.nx - 1 ? phi[p - 2 * plane] : T(0));
+        if (j == 0) {
+            fjp[t] = phi[p + sy];
+            fjm[t] = phi[p + 2 * sy];
+        } else if (j == d.ny - 1) {
+            fjm[t] = phi[p - sy];
+            fjp[t] = phi[p - 2 * sy];
+        } else {
+            fjp[t] = phi[p + sy];
+            fjm[t] = phi[p - sy];
+        }
+        if (k == 0) {
+            fkp[t] = phi[p + 1];
+            fkm[t] = phi[p + 2];
+        } else if (k == d.nz - 1) {
+            fkm[t] = phi[p - 1];
+            fkp[t] = phi[p - 2];
+        } else {
+            fkp[t] = phi[p + 1];
+            fkm[t] = phi[p - 1];
+        }
+        gv[t] = g[p];
+#pragma unroll
+        for (int cmp = 0; cmp < 3; ++cmp) bv0[t][cmp] = b3[cmp * n + p];
+    }
+#pragma unroll
+    for (int t = 0; t < NI; ++t) {
+        if (t >= cnt) break;
+        const int i = i0 + t;
+        const long long p = p0 + (long long)t * plane;
+        const T fm = fi[t], f0 = fi[t + 1], fp = fi[t + 2];
         T gr[3];
-        if (i == 0) gr[0] = (T(4) * fp - T(3) * f0 - phi[p + 2 * plane]) / two_hx;
-        else if (i == d.nx - 1) gr[0] = (T(3) * f0 - T(4) * fm + phi[p - 2 * plane]) / two_hx;
+        if (i == 0) gr[0] = (T(4) * fp - T(3) * f0 - fi2[t]) / two_hx;
+        else if (i == d.nx - 1) gr[0] = (T(3) * f0 - T(4) * fm + fi2[t]) / two_hx;
         else gr[0] = (fp - fm) / two_hx;
-        if (j == 0) gr[1] = (T(4) * phi[p + sy] - T(3) * f0 - phi[p + 2 * sy]) / two_hy;
-        else if (j == d.ny - 1) gr[1] = (T(3) * f0 - T(4) * phi[p - sy] + phi[p - 2 * sy]) / two_hy;
-        else gr[1] = (phi[p + sy] - phi[p - sy]) / two_hy;
-        if (k == 0) gr[2] = (T(4) * phi[p + 1] - T(3) * f0 - phi[p + 2]) / two_hz;
-        else if (k == d.nz - 1) gr[2] = (T(3) * f0 - T(4) * phi[p - 1] + phi[p - 2]) / two_hz;
-        else gr[2] = (phi[p + 1] - phi[p - 1]) / two_hz;
-        const T gg = g[p];
+        // j == 0: fjp = phi(j+1), fjm = phi(j+2); j == ny-1: fjm = phi(j-1), fjp = phi(j-2)
+        if (j == 0) gr[1] = (T(4) * fjp[t] - T(3) * f0 - fjm[t]) / two_hy;
+        else if (j == d.ny - 1) gr[1] = (T(3) * f0 - T(4) * fjm[t] + fjp[t]) / two_hy;
+        else gr[1] = (fjp[t] - fjm[t]) / two_hy;
+        if (k == 0) gr[2] = (T(4) * fkp[t] - T(3) * f0 - fkm[t]) / two_hz;
+        else if (k == d.nz - 1) gr[2] = (T(3) * f0 - T(4) * fkm[t] + fkp[t]) / two_hz;
+        else gr[2] = (fkp[t] - fkm[t]) / two_hz;
+        const T gg = gv[t];
 #pragma unroll
         for (int cmp = 0; cmp < 3; ++cmp) {
-            T bv = b3[cmp * n + p];
+            T bv = bv0[t][cmp];
             bv += gr[cmp];
             const T mag = fabs(bv) - gg;
             const T sgn = T((int)(bv > T(0)) - (int)(bv < T(0)));
@@ -1492,8 +1549,6 @@ __device__ __forceinline__ void bregman_body(const uint3 blockIdx, const dim3 gr
             b3[cmp * n + p] = bv;
             dmb[cmp * n + p] = dn - bv;
         }
-        fm = f0;
-        f0 = fp;
     }
 }
 
