@@ -2509,9 +2509,9 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
     if (nvol == 0) return IM3D_OK;
     if (streams <= 0) streams = 4;
     if (streams > 32) streams = 32;
-    if (ctx->batch_mode != IM3D_BATCH_STREAMS) {
-        // the work list runs valid volumes only; otherwise the stream queue reports each
-        // bad volume and segments the others
+    if (ctx->batch_mode == IM3D_BATCH_WORKLIST) {
+        // the work list runs valid volumes only (the stream queue, the default, reports
+        // each bad volume and segments the others)
         int st = check_params(ctx, p);
         for (int v = 0; v < nvol && st == IM3D_OK; ++v) {
             if (!vols[v].myim || !vols[v].phi_out)
@@ -2520,15 +2520,12 @@ int rsfe_apply_batched(im3d_ctx* ctx, int nvol, const im3d_volume_desc* vols,
                 st = check_dims(ctx, vols[v].nx, vols[v].ny, vols[v].nz, vols[v].hx, vols[v].hy, vols[v].hz);
         }
         int nh = 0;
-        if (st == IM3D_OK && worklist_eligible<T>(p, nvol, vols, &nh))
-            return rsfe_apply_worklist<T>(ctx, nvol, vols, p, nh, streams, stats, latency_ms);
-        if (ctx->batch_mode == IM3D_BATCH_WORKLIST) {
-            if (st != IM3D_OK) return st;
+        if (st != IM3D_OK) return st;
+        if (!worklist_eligible<T>(p, nvol, vols, &nh))
             return fail(ctx, IM3D_ERR_UNSUPPORTED, "the work-list batch needs a residual solve with omega 1, "
                                                    "19 or 25 Gaussian taps on every axis and no "
                                                    "connected-component extraction");
-        }
-        ctx->err.clear();
+        return rsfe_apply_worklist<T>(ctx, nvol, vols, p, nh, streams, stats, latency_ms);
     }
     if (streams > nvol) streams = nvol;
     IM3D_TRY(ensure_workers(ctx, streams));

@@ -789,7 +789,7 @@ def main():
                          "volume, sigma 4, 200 iterations; batch: 48 uneven volumes")
     ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent streams")
     ap.add_argument("--batch-mode", default="auto", choices=["auto", "streams", "worklist"],
-                    help="batch workload: work list (auto picks it for this workload) or stream queue")
+                    help="batch workload: stream queue (auto, the faster) or work list")
     ap.add_argument("--size", type=int, default=0,
                     help="profiling only: cube side of a smaller/larger case (default 256)")
     ap.add_argument("--maxiter", type=int, default=0,

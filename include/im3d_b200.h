@@ -145,10 +145,10 @@ int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
  *                                allocates (0, the default, = no limit). For callers that
  *                                share the GPU under a memory budget.
  *  IM3D_OPT_BATCH_MODE           how im3d_rsfe_apply_batched_* runs its volumes:
- *                                IM3D_BATCH_AUTO (default) = the work list whenever the
- *                                parameters allow it, else the stream queue;
- *                                IM3D_BATCH_STREAMS = the stream queue; IM3D_BATCH_WORKLIST
- *                                = the work list, IM3D_ERR_UNSUPPORTED where it cannot run.
+ *                                IM3D_BATCH_AUTO (default) and IM3D_BATCH_STREAMS = the
+ *                                stream queue (the faster on B200: each volume's state stays
+ *                                in L2 across its stages and sweeps); IM3D_BATCH_WORKLIST =
+ *                                the work list, IM3D_ERR_UNSUPPORTED where it cannot run.
  * Returns IM3D_ERR_INVALID_ARG for an unknown option or a negative value. */
 #define IM3D_OPT_FIT_CHUNKS 1
 #define IM3D_OPT_DEVICE_MEMORY_LIMIT 2
@@ -396,7 +396,7 @@ typedef struct im3d_volume_desc {
 } im3d_volume_desc;
 
 /* Segments nvol volumes with the same parameters, in one of two ways
- * (IM3D_OPT_BATCH_MODE):
+ * (IM3D_OPT_BATCH_MODE; the stream queue by default):
  *  - the work list: groups of up to 64 volumes, largest first, advance their outer
  *    iterations together; each convolution, clamp, Bregman and div stage is ONE
  *    launch over the blocks of every volume of the group, and the Poisson solves run
