@@ -943,11 +943,13 @@ template <typename T>
 __device__ __forceinline__ T grad_term(const T* f, long long p, long long stride, int pos,
                                        int len, double h)
 {
+    // FP32 multiplies by 1/(2h) as the vectorised kernels do (over_two_h); FP64 divides
+    const T two_h = T(2. * h), inv_two_h = T(1. / (2. * h));
     if (pos == 0)
-        return (T(4) * f[p + stride] - T(3) * f[p] - f[p + 2 * stride]) / T(2. * h);
+        return over_two_h(T(4) * f[p + stride] - T(3) * f[p] - f[p + 2 * stride], two_h, inv_two_h);
     if (pos == len - 1)
-        return (T(3) * f[p] - T(4) * f[p - stride] + f[p - 2 * stride]) / T(2. * h);
-    return (f[p + stride] - f[p - stride]) / T(2. * h);
+        return over_two_h(T(3) * f[p] - T(4) * f[p - stride] + f[p - 2 * stride], two_h, inv_two_h);
+    return over_two_h(f[p + stride] - f[p - stride], two_h, inv_two_h);
 }
 
 template <typename T>
@@ -1480,6 +1482,7 @@ __device__ __forceinline__ void bregman_body(const uint3 blockIdx, const dim3 gr
     const long long sy = d.nz;
     const long long p0 = d.idx(i0, j, k);
     const T two_hx = T(2. * hx), two_hy = T(2. * hy), two_hz = T(2. * hz);
+    const T ihx = T(1. / (2. * hx)), ihy = T(1. / (2. * hy)), ihz = T(1. / (2. * hz));
     // Every load of the NI planes is issued before the first store (the stores to b3
     // and dmb would otherwise hold the next plane's loads back): phi along i for planes
     // i0-1 .. i0+NI (and the second one-sided point on an i face), the j and k
@@ -1527,16 +1530,16 @@ __device__ __forceinline__ void bregman_body(const uint3 blockIdx, const dim3 gr
         const long long p = p0 + (long long)t * plane;
         const T fm = fi[t], f0 = fi[t + 1], fp = fi[t + 2];
         T gr[3];
-        if (i == 0) gr[0] = (T(4) * fp - T(3) * f0 - fi2[t]) / two_hx;
-        else if (i == d.nx - 1) gr[0] = (T(3) * f0 - T(4) * fm + fi2[t]) / two_hx;
-        else gr[0] = (fp - fm) / two_hx;
+        if (i == 0) gr[0] = over_two_h(T(4) * fp - T(3) * f0 - fi2[t], two_hx, ihx);
+        else if (i == d.nx - 1) gr[0] = over_two_h(T(3) * f0 - T(4) * fm + fi2[t], two_hx, ihx);
+        else gr[0] = over_two_h(fp - fm, two_hx, ihx);
         // j == 0: fjp = phi(j+1), fjm = phi(j+2); j == ny-1: fjm = phi(j-1), fjp = phi(j-2)
-        if (j == 0) gr[1] = (T(4) * fjp[t] - T(3) * f0 - fjm[t]) / two_hy;
-        else if (j == d.ny - 1) gr[1] = (T(3) * f0 - T(4) * fjm[t] + fjp[t]) / two_hy;
-        else gr[1] = (fjp[t] - fjm[t]) / two_hy;
-        if (k == 0) gr[2] = (T(4) * fkp[t] - T(3) * f0 - fkm[t]) / two_hz;
-        else if (k == d.nz - 1) gr[2] = (T(3) * f0 - T(4) * fkm[t] + fkp[t]) / two_hz;
-        else gr[2] = (fkp[t] - fkm[t]) / two_hz;
+        if (j == 0) gr[1] = over_two_h(T(4) * fjp[t] - T(3) * f0 - fjm[t], two_hy, ihy);
+        else if (j == d.ny - 1) gr[1] = over_two_h(T(3) * f0 - T(4) * fjm[t] + fjp[t], two_hy, ihy);
+        else gr[1] = over_two_h(fjp[t] - fjm[t], two_hy, ihy);
+        if (k == 0) gr[2] = over_two_h(T(4) * fkp[t] - T(3) * f0 - fkm[t], two_hz, ihz);
+        else if (k == d.nz - 1) gr[2] = over_two_h(T(3) * f0 - T(4) * fkm[t] + fkp[t], two_hz, ihz);
+        else gr[2] = over_two_h(fkp[t] - fkm[t], two_hz, ihz);
         const T gg = gv[t];
 #pragma unroll
         for (int cmp = 0; cmp < 3; ++cmp) {

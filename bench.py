@@ -304,7 +304,11 @@ def run_gpu(args):
     pkg = importlib.import_module("3dimagetoolkit_b200")
 
     wl = WORKLOADS[args.workload]
-    shape = wl["shape"] if not args.size else (args.size,) * 3
+    if args.size:
+        dims = [int(v) for v in args.size.split(",")]
+        shape = tuple(dims) if len(dims) == 3 else (dims[0],) * 3
+    else:
+        shape = wl["shape"]
     n = shape[0] * shape[1] * shape[2]
     if args.workload == "c3" and not args.size:
         u0_np, phi0_np = pkg.synth.config_volume("c3", seed=args.seed + rank, dtype=np.float32)
@@ -790,8 +794,8 @@ def main():
     ap.add_argument("--streams", type=int, default=4, help="batch workload: concurrent streams")
     ap.add_argument("--batch-mode", default="auto", choices=["auto", "streams", "worklist"],
                     help="batch workload: stream queue (auto, the faster) or work list")
-    ap.add_argument("--size", type=int, default=0,
-                    help="profiling only: cube side of a smaller/larger case (default 256)")
+    ap.add_argument("--size", type=str, default="",
+                    help="profiling only: cube side (256) or NX,NY,NZ of a smaller/larger case")
     ap.add_argument("--maxiter", type=int, default=0,
                     help="profiling only: outer iterations per step (default 100)")
     args = ap.parse_args()
