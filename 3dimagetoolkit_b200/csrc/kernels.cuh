@@ -1406,7 +1406,7 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
 }
 
 template <typename T, int NI>
-__global__ void __launch_bounds__(256) rb_residual_vec_kernel(const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
+__global__ void __launch_bounds__(256, 4) rb_residual_vec_kernel(const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
 {
     rb_residual_vec_body<T, NI>(blockIdx, gridDim, U, B, d, c, part, want_beff);
 }
