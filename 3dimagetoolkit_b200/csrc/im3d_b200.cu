@@ -690,13 +690,14 @@ constexpr int kNV = 2;  // planes per thread of the vectorised kernels (measured
 constexpr int kNVres = 2;  // planes per thread of the residual check
 const dim3 kBlkVec(32, 4, 1);
 
-// vector groups of 16 bytes along the packed rows, ni planes per thread
+// half-sweep and residual grid: the (vector group, row) pairs of a plane flattened over
+// x blocks
 template <typename T>
-dim3 grid_vec_pk(const Dims& d, dim3 blk, int zmul = 1, int ni = kNV)
+dim3 grid_rb_flat(const Dims& d, dim3 blk, int zmul = 1, int ni = kNV)
 {
-    const int groups = d.hz() / V16<T>::W;
-    return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y,
-                ((d.nx + ni - 1) / ni) * zmul);
+    const long long pairs = (long long)(d.hz() / V16<T>::W) * d.ny;
+    const long long per = (long long)blk.x * blk.y;
+    return dim3((unsigned)((pairs + per - 1) / per), 1, ((d.nx + ni - 1) / ni) * zmul);
 }
 
 template <typename T>
@@ -741,7 +742,7 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
     // the b_eff solve (no own value, omega 1) gets instantiations without the unused
     // paths; with Dirichlet conditions and FP32 it fits 8 blocks per SM
     const bool self = use_self || omega != 1.0;
-    const dim3 grid = grid_vec_pk<T>(d, kBlkVec);
+    const dim3 grid = grid_rb_flat<T>(d, kBlkVec);
     for (int color = 0; color < 2; ++color) {
         const int pf = prof_begin(ctx, "rb_half");
         // red walks the planes forward, black backward: each half-sweep starts on the
@@ -819,7 +820,7 @@ template <typename T>
 int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<T>& c,
              double* beff2, double* rel)
 {
-    const dim3 grid = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
+    const dim3 grid = grid_rb_flat<T>(d, kBlkVec, 2, kNVres);
     const int nvals = *beff2 < 0 ? 2 : 1;
     double* part = nullptr;
     IM3D_TRY(part_buf(ctx, grid, nvals, &part));
@@ -2111,7 +2112,7 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
                                  dsc.nx, dsc.ny, dsc.nz, dsc.hx, dsc.hy, dsc.hz, p, nullptr, nullptr,
                                  nullptr, nullptr, nullptr);
         const Dims& d = V[q].d;
-        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
+        const dim3 gr = grid_rb_flat<T>(d, kBlkVec, 2, kNVres);
         const bool vec = d.nz % V16<T>::W == 0;
         const dim3 gc = vec ? grid_vec<T>(d, kBlkVec) : grid_col(d, kBlkVol);
         if (st == IM3D_OK)
@@ -2187,13 +2188,13 @@ int worklist_group(im3d_ctx* ctx, const std::vector<int>& ids, const im3d_volume
         } else {
             jfw.h.push_back({FitW{v.W2, v.P1, v.f1_d, v.f2_d, d, v.tp.w[0], l1, l2}, fit_win_grid<T>(d)});
         }
-        const dim3 gpk = grid_vec_pk<T>(d, kBlkVec);
+        const dim3 gpk = grid_rb_flat<T>(d, kBlkVec);
         for (int c = 0; c < 2; ++c) {
             // red walks the planes forward, black backward (rb_sweep)
             jrd[c].h.push_back({RbD{v.upk, v.bpk, d, v.coef, c, c}, gpk});
             jrn[c].h.push_back({RbN{v.upk, v.bpk, d, v.coef, c, c}, gpk});
         }
-        const dim3 gr = grid_vec_pk<T>(d, kBlkVec, 2, kNVres);
+        const dim3 gr = grid_rb_flat<T>(d, kBlkVec, 2, kNVres);
         jres.h.push_back({Res{v.upk, v.bpk, d, v.coef, part_res[q]}, gr});
         fin_res[q] = FinalizeJob{part_res[q], (long long)gr.x * gr.y * gr.z, ctrl[q].sum};
         vecrow[q] = d.nz % V16<T>::W == 0;

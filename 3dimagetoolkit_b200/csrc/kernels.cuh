@@ -1203,8 +1203,20 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
     // one drains (both are no-ops in an ordinary launch).
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    // The (vector group, row j) pairs of a block of planes are flattened over the grid's
+    // x blocks, so that no lane idles when a packed row's groups are not a multiple of
+    // blockDim.x (40 groups at nz = 320 left 24 of every 64 lanes idle). A row of exactly
+    // blockDim.x groups (nz = 256) keeps the plain mapping, without the division.
+    const unsigned groups = (unsigned)(d.hz() / W);
+    int g, j;
+    if (groups == blockDim.x) {
+        g = threadIdx.x;
+        j = blockIdx.x * blockDim.y + threadIdx.y;
+    } else {
+        const unsigned lin = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+        g = (int)(lin % groups);
+        j = (int)(lin / groups);
+    }
     const int i0 = (reverse ? gridDim.z - 1 - blockIdx.z : blockIdx.z) * NI;
     const int hz = d.hz();
     const int m0 = g * W;
@@ -1331,8 +1343,17 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    // (vector group, row) pairs flattened over the x blocks as in rb_half_vec_body
+    const unsigned groups = (unsigned)(d.hz() / W);
+    int g, j;
+    if (groups == blockDim.x) {
+        g = threadIdx.x;
+        j = blockIdx.x * blockDim.y + threadIdx.y;
+    } else {
+        const unsigned lin = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+        g = (int)(lin % groups);
+        j = (int)(lin / groups);
+    }
     const int color = blockIdx.z & 1;
     const int i0 = (blockIdx.z >> 1) * NI;
     const int hz = d.hz();
