@@ -700,11 +700,13 @@ dim3 grid_rb_flat(const Dims& d, dim3 blk, int zmul = 1, int ni = kNV)
     return dim3((unsigned)((pairs + per - 1) / per), 1, ((d.nx + ni - 1) / ni) * zmul);
 }
 
+// natural-layout vectorised kernels: (vector group, row) pairs flattened over x blocks
 template <typename T>
 dim3 grid_vec(const Dims& d, dim3 blk)
 {
-    const int groups = d.nz / V16<T>::W;
-    return dim3((groups + blk.x - 1) / blk.x, (d.ny + blk.y - 1) / blk.y, (d.nx + kNV - 1) / kNV);
+    const long long pairs = (long long)(d.nz / V16<T>::W) * d.ny;
+    const long long per = (long long)blk.x * blk.y;
+    return dim3((unsigned)((pairs + per - 1) / per), 1, (d.nx + kNV - 1) / kNV);
 }
 
 dim3 grid_col(const Dims& d, dim3 blk, int ni = kNI)

@@ -1181,6 +1181,22 @@ __device__ __forceinline__ double gs_residual_fp64(const GsCoef<T>& c, const Dim
 }
 
 
+// The (vector group g, row j) pairs of a block of planes, flattened over the grid's x
+// blocks, so that no lane idles when a row's `groups` are not a multiple of blockDim.x
+// (40 groups at nz = 320 left 24 of every 64 lanes idle). A power-of-two number of
+// groups (nz = 256) takes shifts instead of the division.
+__device__ __forceinline__ void flat_pair(const uint3 blockIdx, unsigned groups, int& g, int& j)
+{
+    const unsigned lin = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+    if ((groups & (groups - 1)) == 0) {
+        g = (int)(lin & (groups - 1));
+        j = (int)(lin >> (__ffs((int)groups) - 1));
+    } else {
+        g = (int)(lin % groups);
+        j = (int)(lin / groups);
+    }
+}
+
 // Vectorised red-black half sweep: one thread per group of W = 16/sizeof(T)
 // consecutive packed points (m0 .. m0+W-1) of row j, marching over NI planes of i.
 // All points of a packed row share the parity of k, so their k neighbours are the
@@ -1203,20 +1219,8 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
     // one drains (both are no-ops in an ordinary launch).
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    // The (vector group, row j) pairs of a block of planes are flattened over the grid's
-    // x blocks, so that no lane idles when a packed row's groups are not a multiple of
-    // blockDim.x (40 groups at nz = 320 left 24 of every 64 lanes idle). A row of exactly
-    // blockDim.x groups (nz = 256) keeps the plain mapping, without the division.
-    const unsigned groups = (unsigned)(d.hz() / W);
     int g, j;
-    if (groups == blockDim.x) {
-        g = threadIdx.x;
-        j = blockIdx.x * blockDim.y + threadIdx.y;
-    } else {
-        const unsigned lin = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-        g = (int)(lin % groups);
-        j = (int)(lin / groups);
-    }
+    flat_pair(blockIdx, (unsigned)(d.hz() / W), g, j);
     const int i0 = (reverse ? gridDim.z - 1 - blockIdx.z : blockIdx.z) * NI;
     const int hz = d.hz();
     const int m0 = g * W;
@@ -1343,17 +1347,8 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
-    // (vector group, row) pairs flattened over the x blocks as in rb_half_vec_body
-    const unsigned groups = (unsigned)(d.hz() / W);
     int g, j;
-    if (groups == blockDim.x) {
-        g = threadIdx.x;
-        j = blockIdx.x * blockDim.y + threadIdx.y;
-    } else {
-        const unsigned lin = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
-        g = (int)(lin % groups);
-        j = (int)(lin / groups);
-    }
+    flat_pair(blockIdx, (unsigned)(d.hz() / W), g, j);
     const int color = blockIdx.z & 1;
     const int i0 = (blockIdx.z >> 1) * NI;
     const int hz = d.hz();
@@ -1594,8 +1589,8 @@ __device__ __forceinline__ void clamp_tol_vec_body(const uint3 blockIdx, const d
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int g, j;
+    flat_pair(blockIdx, (unsigned)(d.nz / W), g, j);
     const int i0 = blockIdx.z * NI;
     const int kb = g * W;
     double s_d = 0, s_o = 0;
@@ -1655,8 +1650,8 @@ __device__ __forceinline__ void bregman_vec_body(const uint3 blockIdx, const dim
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int g, j;
+    flat_pair(blockIdx, (unsigned)(d.nz / W), g, j);
     const int i0 = blockIdx.z * NI;
     const int kb = g * W;
     if (kb >= d.nz || j >= d.ny) return;
@@ -1775,8 +1770,8 @@ __device__ __forceinline__ void div_vec_body(const uint3 blockIdx, const dim3 gr
     typedef V16<T> VT;
     typedef typename VT::type VV;
     constexpr int W = VT::W;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int g, j;
+    flat_pair(blockIdx, (unsigned)(d.nz / W), g, j);
     const int i0 = blockIdx.z * NI;
     const int kb = g * W;
     if (kb >= d.nz || j >= d.ny) return;
