@@ -30,10 +30,11 @@ FP32_BOUNDS = {"u": 1e-5, "f1": 1e-5, "f2": 1e-5}
 
 PARAMS = dict(sigma=3.0, lamda1=1.0, lamda2=1.0, epsilon=1e-3, lamda=0.5, bc=2, tol=0.0,
               gs_rel_res_tol=1e-6, gs_max_sweeps=1000)
-# workload, outer iterations, bounds on the relative L2 of (u, f1, f2)
+# workload, outer iterations, bounds on the relative L2 of (u, f1, f2); at 512x512x320
+# (200 outer iterations) the FP32 run measured 4.0e-5, 1.1e-5 and 8.6e-6
 CASES = [("c2", dict(maxiter=10), (1e-5, 1e-5, 1e-5)),
          ("c2", dict(maxiter=100), (1e-5, 1e-5, 1e-5)),
-         ("c3", dict(maxiter=200, sigma=4.0), (5e-3, 1.5e-3, 1.5e-3))]
+         ("c3", dict(maxiter=200, sigma=4.0), (2e-4, 5e-5, 5e-5))]
 
 
 @pytest.mark.parametrize("name, kw, bounds", CASES)
