@@ -32,7 +32,7 @@ ERR_NONFINITE = 8
 
 BC_DEFAULT, BC_NEU, BC_DIR = 0, 1, 2
 SWEEP_LEXICOGRAPHIC, SWEEP_REDBLACK = 0, 1
-OPT_FIT_CHUNKS, OPT_DEVICE_MEMORY_LIMIT, OPT_BATCH_MODE = 1, 2, 3
+OPT_FIT_CHUNKS, OPT_DEVICE_MEMORY_LIMIT, OPT_BATCH_MODE, OPT_TILE_LOADS = 1, 2, 3, 4
 BATCH_AUTO, BATCH_STREAMS, BATCH_WORKLIST = 0, 1, 2
 WS_OFF, WS_PREDICT, WS_TRAIN = 0, 1, 2
 
@@ -241,8 +241,8 @@ class Context:
         self._check(lib().im3d_ctx_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 
     def set_option(self, option: int, value: int):
-        """im3d_ctx_set_option: OPT_FIT_CHUNKS, OPT_DEVICE_MEMORY_LIMIT (bytes) or
-        OPT_BATCH_MODE (BATCH_AUTO, BATCH_STREAMS, BATCH_WORKLIST)."""
+        """im3d_ctx_set_option: OPT_FIT_CHUNKS, OPT_DEVICE_MEMORY_LIMIT (bytes),
+        OPT_BATCH_MODE (BATCH_AUTO, BATCH_STREAMS, BATCH_WORKLIST) or OPT_TILE_LOADS (0, 1)."""
         self._check(lib().im3d_ctx_set_option(self._h, C.c_int(option), C.c_int64(value)))
 
     def set_observer(self, every: int, fn=None, with_state: bool = False, dtype=np.float64):

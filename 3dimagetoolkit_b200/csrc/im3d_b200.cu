@@ -21,8 +21,11 @@
 #include "../../include/im3d_b200.h"
 #include "common.cuh"
 #include "internal.h"
+#include "conv_tma.cuh"
 #include "kernels.cuh"
 #include "worklist.cuh"
+
+#include <cudaTypedefs.h>
 
 using namespace im3d;
 
@@ -75,6 +78,7 @@ struct im3d_ctx {
     int wl_ctrl_cap = 0;
     cudaEvent_t wl_ev[2] = {nullptr, nullptr};  // work-list solve phase: start, this worker done
     int batch_mode = IM3D_BATCH_AUTO;
+    int tile_loads = 1;  // the FP32 Heaviside pass moves its rows with TMA where it can
     int num_sms = 148;
     int ifit_chunks = 0;  // i chunks of the marching fit stage (0: cost model)
     size_t mem_limit = 0;  // device bytes the context may hold in buffers (0: no limit)
@@ -448,6 +452,94 @@ int pass_k(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, int nh,
     dim3 grid((unsigned)((rows + RK - 1) / RK), (d.nz + TK - 1) / TK);
     const int pf = prof_begin(ctx, name);
     kern<<<grid, dim3(TK, RK), smem, ctx->stream>>>(ld, st, d, w, nh);
+    prof_end(ctx, pf);
+    return check_launch(ctx, name);
+}
+
+// ------------------------------------------- Heaviside pass with TMA-moved rows (FP32)
+// cuTensorMapEncodeTiled of the driver, resolved once.
+[[maybe_unused]] PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// Whether the TMA pass takes this volume: FP32 rows of a multiple of 8 cells, at most 256
+// (one box), 16-byte aligned buffers, 19 or 25 taps.
+[[maybe_unused]] inline bool heav_tma_eligible(const im3d_ctx* ctx, const Dims& d, int nh, const void* phi,
+                                               const void* u0, const void* out)
+{
+    auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    return ctx->tile_loads && (nh == 19 || nh == 25) && d.nz % 8 == 0 && d.nz <= 256 && al(phi) && al(u0) &&
+           al(out) && (long long)d.nx * d.ny < (1ll << 31);
+}
+
+// The Heaviside pass (LdHeaviside + StVec<float, 4>) on conv_k_heav_tma_kernel, 4 rows per
+// block (measured at 256^3: 4 rows as fast as conv_k_win_kernel or faster; 2 and 8 rows
+// slower).
+template <int S>
+int pass_heav_tma(im3d_ctx* ctx, const float* phi, const float* u0, Vec<float, 4>* out, const Dims& d,
+                  const float* taps, float center, float inv_eps, const char* name)
+{
+    constexpr int RB = 4;
+    auto enc = tmap_encoder();
+    if (!enc) return fail(ctx, IM3D_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const int KB = (d.nz + 15) & ~15;
+    const long long rows = (long long)d.nx * d.ny;
+    const size_t smem = HeavTmaLayout<RB, S>::total(KB);
+    auto kern = conv_k_heav_tma_kernel<RB, S>;
+    IM3D_TRY(set_smem(ctx, kern, smem));
+    int occ = 0;
+    IM3D_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, RB * 32, smem));
+    if (occ < 1) return fail(ctx, IM3D_ERR_UNSUPPORTED, "the TMA Heaviside pass does not fit an SM");
+    CUtensorMap mp, mu, mo;
+    {
+        cuuint64_t dims[2] = {(cuuint64_t)d.nz, (cuuint64_t)rows};
+        cuuint64_t str[1] = {(cuuint64_t)d.nz * 4};
+        cuuint32_t box[2] = {(cuuint32_t)KB, (cuuint32_t)RB};
+        cuuint32_t es[2] = {1, 1};
+        for (int f = 0; f < 2; ++f) {
+            const CUresult r = enc(f ? &mu : &mp, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                                   const_cast<float*>(f ? u0 : phi), dims, str, box, es,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS)
+                return fail(ctx, IM3D_ERR_CUDA, "cuTensorMapEncodeTiled (rows) failed: " + std::to_string((int)r));
+        }
+    }
+    {
+        // the output viewed as rows x (nz / 8) groups x 32 floats (8 cells of 4 fields)
+        cuuint64_t dims[3] = {32, (cuuint64_t)(d.nz / 8), (cuuint64_t)rows};
+        cuuint64_t str[2] = {128, (cuuint64_t)d.nz * 16};
+        cuuint32_t box[3] = {32, (cuuint32_t)(KB / 8), (cuuint32_t)RB};
+        cuuint32_t es[3] = {1, 1, 1};
+        const CUresult r = enc(&mo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, reinterpret_cast<float*>(out), dims, str,
+                               box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return fail(ctx, IM3D_ERR_CUDA, "cuTensorMapEncodeTiled (cells) failed: " + std::to_string((int)r));
+    }
+    HeavTmaArgs a;
+    a.d = d;
+    a.taps = taps;
+    a.center = center;
+    a.inv_eps = inv_eps;
+    a.KB = KB;
+    a.nrb = (rows + RB - 1) / RB;
+    a.err = &ctx->ctrl_d->flag[0];
+    const long long G = std::min<long long>(a.nrb, (long long)occ * ctx->num_sms);
+    const int pf = prof_begin(ctx, name);
+    kern<<<(unsigned)G, RB * 32, smem, ctx->stream>>>(mp, mu, mo, a);
     prof_end(ctx, pf);
     return check_launch(ctx, name);
 }
@@ -1389,8 +1481,19 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
 
     for (t = t0 + 1; tollerance > p->tol && t <= p->maxiter; ++t) {
         // stage 1-5: Heaviside, the four convolutions, fitting terms, forcing term
-        IM3D_TRY((pass_k<T, 4>(ctx, LdHeaviside<T>{phi, u0, d, center, inv_eps}, StVec<T, 4>{W1, d},
-                               d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
+        bool tma_done = false;
+        if constexpr (std::is_same<T, float>::value) {
+            if (heav_tma_eligible(ctx, d, tp.nh[2], phi, u0, W1)) {
+                if (tp.nh[2] == 19)
+                    IM3D_TRY(pass_heav_tma<9>(ctx, phi, u0, W1, d, tp.w[2], center, inv_eps, "conv_k_heaviside"));
+                else
+                    IM3D_TRY(pass_heav_tma<12>(ctx, phi, u0, W1, d, tp.w[2], center, inv_eps, "conv_k_heaviside"));
+                tma_done = true;
+            }
+        }
+        if (!tma_done)
+            IM3D_TRY((pass_k<T, 4>(ctx, LdHeaviside<T>{phi, u0, d, center, inv_eps}, StVec<T, 4>{W1, d},
+                                   d, tp.w[2], tp.nh[2], "conv_k_heaviside")));
         IM3D_TRY((pass_s<T, 4, 1>(ctx, LdVec<T, 4>{W1, d}, StVec<T, 4>{W2, d}, d, tp.w[1], tp.nh[1],
                                   "conv_s_j4")));
         IM3D_TRY(pass_i_fit<T>(ctx, W2, P1, f1_d, f2_d, d, tp.w[0], tp.host[0], tp.nh[0], (T)p->lamda1,
@@ -1565,6 +1668,8 @@ int rsfe_apply(im3d_ctx* ctx, const T* myim_user, const T* init_user, int nx, in
             IM3D_TRY(check_launch(ctx, "div"));
         }
         if (cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) IM3D_TRY(sync(ctx));
+        if (ctx->ctrl_h->flag[0])
+            return fail(ctx, IM3D_ERR_CUDA, "a TMA load of the Heaviside pass did not complete in time");
         tollerance = std::sqrt(hhh * ctx->ctrl_h->sum[SUM_DPHI2]) /
                      std::sqrt(hhh * ctx->ctrl_h->sum[SUM_PHIOLD2]);
         if (lex) std::swap(phi, other);
@@ -1957,6 +2062,7 @@ int ensure_workers(im3d_ctx* ctx, int n)
         if (st != IM3D_OK) return fail(ctx, st, "cannot create a worker context");
         w->mem_limit = ctx->mem_limit;
         w->ifit_chunks = ctx->ifit_chunks;
+        w->tile_loads = ctx->tile_loads;
         ctx->workers.push_back(w);
     }
     for (im3d_ctx* w : ctx->workers) w->prof = 0;
@@ -2697,6 +2803,11 @@ int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value)
     case IM3D_OPT_BATCH_MODE:
         if (value > IM3D_BATCH_WORKLIST) return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown batch mode");
         ctx->batch_mode = (int)value;
+        return IM3D_OK;
+    case IM3D_OPT_TILE_LOADS:
+        if (value > 1) return fail(ctx, IM3D_ERR_INVALID_ARG, "IM3D_OPT_TILE_LOADS is 0 or 1");
+        ctx->tile_loads = (int)value;
+        for (im3d_ctx* w : ctx->workers) w->tile_loads = (int)value;
         return IM3D_OK;
     default:
         return fail(ctx, IM3D_ERR_INVALID_ARG, "unknown option " + std::to_string(option));

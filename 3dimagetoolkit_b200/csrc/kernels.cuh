@@ -31,14 +31,15 @@ __device__ __forceinline__ void heaviside_pair(T phi, T center, T inv_eps, T& H,
     const T inv_pi = T(0.318309886183790671537767526745028724);
     const T x = (phi - center) * inv_eps;
     const T y = fabs(x);
-    T small;
-    if (y >= T(1)) {
-        T inv_y;
-        if constexpr (sizeof(T) == 4) inv_y = __frcp_rn(y);  // = 1.0f / y, correctly rounded
-        else inv_y = T(1) / y;
-        small = atan(inv_y) * inv_pi;
+    // one arctangent, of 1/y or y, and selects instead of branches
+    const bool big = y >= T(1);
+    T arg = y;
+    if (big) {
+        if constexpr (sizeof(T) == 4) arg = __frcp_rn(y);  // = 1.0f / y, correctly rounded
+        else arg = T(1) / y;
     }
-    else small = T(0.5) - atan(y) * inv_pi;
+    const T at = atan(arg);
+    const T small = big ? at * inv_pi : T(0.5) - at * inv_pi;
     const T large = T(1) - small;
     if (x > T(0)) { H = large; Hb = small; }
     else { H = small; Hb = large; }

@@ -88,6 +88,42 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const void* map, uint64_t
         : "memory");
 }
 
+// Tiled TMA load of a 2-D box, completing on `bar`; this GPU's own memory, no multicast.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* map, uint64_t* bar, int c0, int c1)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// Tiled TMA store of a 3-D box from shared memory (bulk-group completion). The parts
+// of the box outside the tensor are not written.
+__device__ __forceinline__ void tma_store_3d(const void* map, const void* src, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(map), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Waits until the committed bulk stores of this thread have read their shared memory.
+__device__ __forceinline__ void bulk_wait_read0()
+{
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Waits until the committed bulk stores of this thread are complete.
+__device__ __forceinline__ void bulk_wait0()
+{
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // Generic-proxy writes to shared memory become visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_proxy_async_smem()
 {

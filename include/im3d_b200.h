@@ -149,6 +149,11 @@ int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
  *                                stream queue (the faster on B200: each volume's state stays
  *                                in L2 across its stages and sweeps); IM3D_BATCH_WORKLIST =
  *                                the work list, IM3D_ERR_UNSUPPORTED where it cannot run.
+ *  IM3D_OPT_TILE_LOADS           1 (default): the FP32 Heaviside pass moves whole rows
+ *                                with the Tensor Memory Accelerator where the volume allows
+ *                                it (nz a multiple of 8 and at most 256, 16-byte aligned
+ *                                buffers, 19 or 25 taps); 0: the register-window kernel
+ *                                everywhere. Both give bit-identical results.
  * Returns IM3D_ERR_INVALID_ARG for an unknown option or a negative value. */
 #define IM3D_OPT_FIT_CHUNKS 1
 #define IM3D_OPT_DEVICE_MEMORY_LIMIT 2
@@ -156,6 +161,7 @@ int64_t im3d_ctx_launch_count(const im3d_ctx* ctx);
 #define IM3D_BATCH_AUTO 0
 #define IM3D_BATCH_STREAMS 1
 #define IM3D_BATCH_WORKLIST 2
+#define IM3D_OPT_TILE_LOADS 4
 int im3d_ctx_set_option(im3d_ctx* ctx, int option, int64_t value);
 /* Per-stage device timing: with profiling on, each launch of the loop's kernels is
  * bracketed by CUDA events on the launching stream. im3d_ctx_profile() synchronises,

@@ -54,6 +54,6 @@ def test_python_constants_match_the_header(pkg):
         if name.startswith(prefixes) and hasattr(pkg._abi, name):
             assert getattr(pkg._abi, name) == int(value), name
             checked += 1
-    for must in ("OPT_BATCH_MODE", "BATCH_AUTO", "BATCH_STREAMS", "BATCH_WORKLIST", "ERR_NONFINITE"):
+    for must in ("OPT_BATCH_MODE", "OPT_TILE_LOADS", "BATCH_AUTO", "BATCH_STREAMS", "BATCH_WORKLIST", "ERR_NONFINITE"):
         assert must in defs and hasattr(pkg._abi, must), must
     assert checked >= 20
