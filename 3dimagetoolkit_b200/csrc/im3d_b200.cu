@@ -848,6 +848,9 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
         else if (c.neu)
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, true>, grid, kBlkVec,
                                       U, B, d, c, color, 0, T(1), reverse));
+        else if (2 * d.npk() < (1ll << 31))
+            IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1, int>,
+                                      grid, kBlkVec, U, B, d, c, color, 0, T(1), reverse));
         else
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1>,
                                       grid, kBlkVec, U, B, d, c, color, 0, T(1), reverse));

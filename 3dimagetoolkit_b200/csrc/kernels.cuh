@@ -1208,8 +1208,9 @@ __device__ __forceinline__ void flat_pair(const uint3 blockIdx, unsigned groups,
 // match). Without both the kernel needs fewer registers and fits MINB blocks per SM.
 // reverse: the blocks take the planes of i from the last to the first, so that a
 // half-sweep following one in the other direction starts on the planes that are still
-// in L2.
-template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
+// in L2. IX: the type of the cell offsets, int where both colours' cells number less
+// than 2^31 (fewer instructions per address), else long long.
+template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1, typename IX = long long>
 __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim3 gridDim, T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, int color, int use_self, T omega, int reverse)
 {
     typedef V16<T> VT;
@@ -1226,13 +1227,13 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
     const int hz = d.hz();
     const int m0 = g * W;
     if (m0 >= hz || j >= d.ny) return;
-    const long long plane = (long long)d.ny * hz;
-    const long long npk = plane * d.nx;
+    const IX plane = (IX)d.ny * hz;
+    const IX npk = plane * d.nx;
     T* own = U + (color ? npk : 0);
     const T* oth = U + (color ? 0 : npk);
     const T* bb = B + (color ? npk : 0);
     const bool jint = j >= 1 && j <= d.ny - 2;
-    const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
+    const IX q0 = ((IX)i0 * d.ny + j) * hz + m0;
     const bool relax = SELF && omega != T(1);
     if (!SELF) use_self = 0;
     // Every load of the NI planes is issued before the first store: the stores go to
@@ -1243,13 +1244,13 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
 #pragma unroll
     for (int t = 0; t < NI + 2; ++t) {
         const int i = i0 - 1 + t;
-        if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (long long)(t - 1) * plane);
+        if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (IX)(t - 1) * plane);
         else o[t] = VV{};
     }
 #pragma unroll
     for (int t = 0; t < NI; ++t) {
         const int i = i0 + t;
-        const long long q = q0 + (long long)t * plane;
+        const IX q = q0 + (IX)t * plane;
         const int par = (i + j + color) & 1;
         ymv[t] = ypv[t] = bvv[t] = sfv[t] = VV{};
         exv[t] = T(0);
@@ -1267,7 +1268,7 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
     for (int t = 0; t < NI; ++t) {
         const int i = i0 + t;
         if (i >= d.nx) break;
-        const long long q = q0 + (long long)t * plane;
+        const IX q = q0 + (IX)t * plane;
         const int par = (i + j + color) & 1;
         const bool rowint = jint && i >= 1 && i <= d.nx - 2;
         if (rowint) {
@@ -1334,10 +1335,10 @@ __device__ __forceinline__ void rb_half_vec_body(const uint3 blockIdx, const dim
     }
 }
 
-template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1>
+template <typename T, int NI, bool SELF = true, bool NEU = true, int MINB = 1, typename IX = long long>
 __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, int color, int use_self, T omega, int reverse = 0)
 {
-    rb_half_vec_body<T, NI, SELF, NEU, MINB>(blockIdx, gridDim, U, B, d, c, color, use_self, omega, reverse);
+    rb_half_vec_body<T, NI, SELF, NEU, MINB, IX>(blockIdx, gridDim, U, B, d, c, color, use_self, omega, reverse);
 }
 
 // Vectorised FP64 residual, same walk as rb_half_vec_kernel; blockIdx.z covers
