@@ -829,6 +829,14 @@ int launch_dependent(im3d_ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 blk,
     return IM3D_OK;
 }
 
+// Whether every cell offset of the solve's two colour-packed fields fits an int (the
+// half-sweep and the residual check then take 32-bit offsets: fewer instructions per
+// address; the streaming kernels measured no gain or a loss from it).
+inline bool fits_int32(const Dims& d)
+{
+    return 2 * d.npk() < (1ll << 31);
+}
+
 template <typename T>
 int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c, int use_self,
              double omega)
@@ -848,7 +856,7 @@ int rb_sweep(im3d_ctx* ctx, T* U, const T* B, const Dims& d, const GsCoef<T>& c,
         else if (c.neu)
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, true>, grid, kBlkVec,
                                       U, B, d, c, color, 0, T(1), reverse));
-        else if (2 * d.npk() < (1ll << 31))
+        else if (fits_int32(d))
             IM3D_TRY(launch_dependent(ctx, rb_half_vec_kernel<T, kNV, false, false, sizeof(T) == 4 ? 8 : 1, int>,
                                       grid, kBlkVec, U, B, d, c, color, 0, T(1), reverse));
         else
@@ -923,7 +931,10 @@ int rb_check(im3d_ctx* ctx, const T* U, const T* B, const Dims& d, const GsCoef<
     IM3D_TRY(part_buf(ctx, grid, nvals, &part));
     ctx->residual_checks++;
     const int pf = prof_begin(ctx, "rb_residual");
-    rb_residual_vec_kernel<T, kNVres><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
+    if (fits_int32(d))
+        rb_residual_vec_kernel<T, kNVres, int><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
+    else
+        rb_residual_vec_kernel<T, kNVres><<<grid, kBlkVec, 0, ctx->stream>>>(U, B, d, c, part, nvals == 2 ? 1 : 0);
     prof_end(ctx, pf);
     IM3D_TRY(check_launch(ctx, "rb_residual"));
     IM3D_TRY(finalize(ctx, part, grid, nvals, SUM_RES2));

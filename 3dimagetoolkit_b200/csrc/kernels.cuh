@@ -1343,7 +1343,7 @@ __global__ void __launch_bounds__(128, MINB) rb_half_vec_kernel(T* __restrict__ 
 
 // Vectorised FP64 residual, same walk as rb_half_vec_kernel; blockIdx.z covers
 // (plane block, colour).
-template <typename T, int NI>
+template <typename T, int NI, typename IX = long long>
 __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const dim3 gridDim, const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
 {
     typedef V16<T> VT;
@@ -1357,26 +1357,26 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
     const int m0 = g * W;
     double acc = 0, accb = 0;
     if (m0 < hz && j < d.ny) {
-        const long long plane = (long long)d.ny * hz;
-        const long long npk = plane * d.nx;
+        const IX plane = (IX)d.ny * hz;
+        const IX npk = plane * d.nx;
         const T* own = U + (color ? npk : 0);
         const T* oth = U + (color ? 0 : npk);
         const T* bb = B + (color ? npk : 0);
         const bool jint = j >= 1 && j <= d.ny - 2;
         const int lo = c.neu ? 0 : 1;
-        const long long q0 = ((long long)i0 * d.ny + j) * hz + m0;
+        const IX q0 = ((IX)i0 * d.ny + j) * hz + m0;
         VV o[NI + 2];
 #pragma unroll
         for (int t = 0; t < NI + 2; ++t) {
             const int i = i0 - 1 + t;
-            if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (long long)(t - 1) * plane);
+            if (i >= 0 && i < d.nx) o[t] = *reinterpret_cast<const VV*>(oth + q0 + (IX)(t - 1) * plane);
             else o[t] = VV{};
         }
 #pragma unroll
         for (int t = 0; t < NI; ++t) {
             const int i = i0 + t;
             if (i >= d.nx) break;
-            const long long q = q0 + (long long)t * plane;
+            const IX q = q0 + (IX)t * plane;
             const int par = (i + j + color) & 1;
             const bool rowint = jint && i >= 1 && i <= d.nx - 2;
             const VV bv = *reinterpret_cast<const VV*>(bb + q);
@@ -1384,7 +1384,7 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
             if (rowint) {
                 const VV ym = *reinterpret_cast<const VV*>(oth + q - hz);
                 const VV yp = *reinterpret_cast<const VV*>(oth + q + hz);
-                const long long qe = par ? q + W : q - 1;
+                const IX qe = par ? q + W : q - 1;
                 const bool e_ok = par ? (m0 + W < hz) : (m0 >= 1);
                 const double extra = e_ok ? (double)oth[qe] : 0.0;
 #pragma unroll
@@ -1423,10 +1423,10 @@ __device__ __forceinline__ void rb_residual_vec_body(const uint3 blockIdx, const
     else block_sum_store(acc, part, block_linear_id(blockIdx, gridDim));
 }
 
-template <typename T, int NI>
+template <typename T, int NI, typename IX = long long>
 __global__ void __launch_bounds__(256, 4) rb_residual_vec_kernel(const T* __restrict__ U, const T* __restrict__ B, Dims d, GsCoef<T> c, double* part, int want_beff)
 {
-    rb_residual_vec_body<T, NI>(blockIdx, gridDim, U, B, d, c, part, want_beff);
+    rb_residual_vec_body<T, NI, IX>(blockIdx, gridDim, U, B, d, c, part, want_beff);
 }
 
 
