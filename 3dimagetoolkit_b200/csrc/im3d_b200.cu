@@ -562,13 +562,18 @@ int pass_s_win(im3d_ctx* ctx, Ld ld, St st, const Dims& d, const T* w, const cha
 {
     constexpr int R = SWinR<T>::v;
     const size_t smem = s_win_smem<T, N, S>();
-    auto kern = conv_s_win_kernel<T, N, AXIS, S, TW, TY, R, Ld, St>;
-    IM3D_TRY(set_smem(ctx, kern, smem));
     const dim3 grid = s_win_grid<T, AXIS>(d);
-    const int pf = prof_begin(ctx, name);
-    kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w);
-    prof_end(ctx, pf);
-    return check_launch(ctx, name);
+    auto run = [&](auto kern) -> int {
+        IM3D_TRY(set_smem(ctx, kern, smem));
+        const int pf = prof_begin(ctx, name);
+        kern<<<grid, dim3(TW, TY), smem, ctx->stream>>>(ld, st, d, w);
+        prof_end(ctx, pf);
+        return check_launch(ctx, name);
+    };
+    if constexpr (kPairedS<T, N>)
+        return run(conv_s_win_pair_kernel<T, N, AXIS, S, TW, TY, R, Ld, St>);
+    else
+        return run(conv_s_win_kernel<T, N, AXIS, S, TW, TY, R, Ld, St>);
 }
 
 template <typename T, int N, int AXIS, class Ld, class St>
