@@ -2058,6 +2058,14 @@ int gauss_filter_noalloc(const float* in, float* out, int nx, int ny, int nz, do
                       LdVec<float, 1>{t2, d}, StScalar<float>{out, d}, d, w, nh[0]) != cudaSuccess)
             return IM3D_ERR_CUDA;
     }
+    // a stream being captured into a graph cannot be synchronized: the graph orders the
+    // work and its launch is the caller's to wait for
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return IM3D_ERR_CUDA;
+    }
+    if (cs != cudaStreamCaptureStatusNone) return IM3D_OK;
     if (cudaStreamSynchronize(stream) != cudaSuccess) {
         cudaGetLastError();
         return IM3D_ERR_CUDA;

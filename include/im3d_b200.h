@@ -239,7 +239,10 @@ int im3d_poisson_solve_f64(im3d_ctx* ctx, double* u, const double* b, int nx, in
  * 2097152 voxels (128^3) return IM3D_ERR_TOO_LARGE, and nx or ny above 65535 return
  * IM3D_ERR_INVALID_ARG, both without touching the GPU. The first call on a device
  * looks the array's device address up (cudaGetSymbolAddress); make that first call
- * before any stream capture. Calls share the array, so calls that overlap on the GPU
+ * before any stream capture. Later calls may be captured into a CUDA graph: on a
+ * capturing stream the call returns without waiting, and the caller waits for the
+ * graph's launch; otherwise it returns after the stream has finished the filter. Calls
+ * share the array, so calls that overlap on the GPU
  * (other threads or streams) race; every call rewrites all of the scratch it reads,
  * so nothing carries over from the previous call. A launch that fails returns
  * IM3D_ERR_CUDA; an error the caller left pending is neither reported nor cleared. */

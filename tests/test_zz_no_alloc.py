@@ -90,3 +90,30 @@ def test_noalloc_filter_refuses_a_launch_geometry_that_does_not_fit():
     out = torch.full_like(x, 5.0)
     assert _noalloc(pkg.lib(), x, out, 1.0, (1.0, 1.0, 1.0)) == 1
     assert bool((out == 5.0).all())  # nothing was written
+
+
+def test_noalloc_filter_captured_in_a_cuda_graph():
+    # the first call (outside any capture) looks the scratch up; a later call captured
+    # into a graph neither waits nor fails, and each replay filters the current input
+    torch = pytest.importorskip("torch")
+    pkg = importlib.import_module("3dimagetoolkit_b200")
+    lib = pkg.lib()
+    shape = (40, 36, 32)
+    x = torch.rand(shape, device="cuda")
+    out = torch.empty_like(x)
+    assert _noalloc(lib, x, out, 2.0, (1.0, 1.0, 1.0)) == 0
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        st = _noalloc(lib, x, out, 2.0, (1.0, 1.0, 1.0), stream=torch.cuda.current_stream().cuda_stream)
+    assert st == 0, st
+    with pkg.Context(0) as ctx:
+        for seed in (1, 2):
+            g = torch.Generator(device="cuda")
+            g.manual_seed(seed)
+            x.copy_(torch.rand(shape, device="cuda", generator=g))
+            out.fill_(float("nan"))
+            graph.replay()
+            torch.cuda.synchronize()
+            want = ctx.gauss_filter(x.cpu().numpy(), 2.0)
+            assert _rel(out.cpu().numpy(), want) < 2e-6, seed
+    del graph
